@@ -1,0 +1,334 @@
+"""Benchmark of the tile-grained mixed-precision single-kernel CG on one or more B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one mixed-precision CG solve of the 3D 7-point variable-coefficient
+Poisson system on 128^3 cells (n = 2,097,152, nnz = 14,581,760, k = exp(N(0,1))
+per face, b = A x_true, x_true ~ U(-1,1)) to a relative residual of 1e-8,
+verified in FP64 on the GPU, with FP64 residual replacement every 50
+iterations.  The input lives in HBM before the timed region; the matrix slice
+payload (hundreds of MB) is larger than the 126 MB L2, so no flush is needed
+between steps.  The same solve in all-FP64, the standalone FP64 tile SpMV (HBM
+GB/s, L2 flushed between launches) and an end-to-end solve through the public
+API with host buffers are reported beside it.
+
+With N GPUs (torchrun) every rank solves its own replica (a single system does
+not shard; replicas only) and value = max-over-ranks time / (N * K).
+
+--impl reference times the reference's CPU path: the FP64 tile-SpMV CG restated
+from the reference (oracle/), on all host threads, one full solve for the
+iteration count, then K bounded samples of iterations.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mille-feuille_b200"))
+
+METRIC = "ms to 1e-8 rel-res, mixed vs FP64 kernel on B200; SpMV HBM GB/s; fwd+adjoint ms"
+WORKLOAD = "poisson3d_varcoef_128: mixed-precision single-kernel CG to 1e-8 rel-res (FP64-verified)"
+TOL = 1e-8
+N_SIDE = 128
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_system():
+    from millefeuille import matrices as M
+    A, b, x_true = M.poisson3d_varcoef(N_SIDE, seed=1)
+    return A, b, x_true
+
+
+def algorithmic_bytes(rep, n, nnz, tilenum, method="cg"):
+    """SpMV bytes: sum_t nnz_t (s_t + 1) + 8 per tile; vectors 96 n per CG
+    iteration (160 n and two SpMVs per BiCGSTAB iteration); each FP64
+    residual replacement streams the FP64 payload plus 24 n."""
+    sizes = (8, 4, 2, 1)
+    mat = sum(c * (s + 1) for c, s in zip(rep["nnz_uses"], sizes)) + 8 * sum(rep["tile_uses"])
+    vec = (96 if method == "cg" else 160) * n * rep["iterations"]
+    repl = rep["replacements"] * (9 * nnz + 8 * tilenum + 24 * n)
+    return mat + vec + repl
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import millefeuille as mf
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    A, b, x_true = make_system()
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    info = G.info
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    bd = torch.from_numpy(b).to(dev)
+    xd = torch.zeros_like(bd)
+    mixed = mf.default_options(precision="mixed", tol=TOL)
+    fp64 = mf.default_options(precision="fp64", tol=TOL, replace_every=0)
+
+    def sync_all():
+        torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
+
+    def timed(opt, steps, host=False):
+        reps = []
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        hb = b.copy()
+        hx = np.zeros_like(hb)
+        sync_all()
+        ev0.record(stream)
+        for _ in range(steps):
+            if host:
+                _, r = G.solve(hb, hx, options=opt, stream=sp)
+            else:
+                _, r = G.solve(bd, xd, options=opt, stream=sp)
+            reps.append(r)
+        ev1.record(stream)
+        sync_all()
+        ms = ev0.elapsed_time(ev1) / steps
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, reps
+
+    for _ in range(args.warmup):
+        G.solve(bd, xd, options=mixed, stream=sp)
+    with ClockSampler(local_rank) as clk:
+        ms_mixed, reps = timed(mixed, args.steps)
+    rep = reps[-1]
+    # the same kernel in all-FP64
+    G.solve(bd, xd, options=fp64, stream=sp)
+    ms_fp64, reps64 = timed(fp64, max(1, args.steps))
+    rep64 = reps64[-1]
+    # end to end through the public API with host buffers (H2D b, D2H x each step)
+    G.solve(b, np.zeros_like(b), options=mixed, stream=sp)
+    ms_e2e, _ = timed(mixed, args.steps, host=True)
+    # standalone FP64 tile SpMV, L2 flushed between launches
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    xs = torch.from_numpy(np.random.default_rng(7).uniform(-1, 1, A.n)).to(dev)
+    ys = torch.empty_like(xs)
+    spmv_ms = []
+    for i in range(args.warmup + 10):
+        flush.fill_(float(i))
+        G.spmv(xs, ys, precision="fp64", stream=sp)
+        if i >= args.warmup:
+            spmv_ms.append(G.last_spmv_ms)
+    spmv_t = statistics.median(spmv_ms)
+    n, nnz, T = A.n, A.nnz, info["tilenum"]
+    b_spmv = 9 * nnz + 8 * T + 16 * n
+    peak, peak_kind = _peaks()
+    alg = algorithmic_bytes(rep, n, nnz, T)
+    achieved = alg / (rep["time_ms"] * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "solve_mixed_poisson3d_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    # independent FP64 check of the returned solution (host, scipy)
+    x = xd.cpu().numpy()
+    relres_host = float(np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b))
+    value = ms_mixed / world
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_mixed, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 dots/updates, f32/f16/i8 tile products",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {
+            "workload": WORKLOAD, "n": n, "nnz": nnz, "tiles": T, "tol": TOL, "replace_every": 50,
+            "parallelism": f"replicas x{world} (one system per GPU)",
+            "l2": f"inputs larger than L2: slice payload {round(info['slice_entries'] * 16 / 1e6)} MB per solve",
+            "iterations_mixed": rep["iterations"], "relres_true_mixed": rep["relres_true"],
+            "relres_host_check": relres_host, "fp64_ms": round(ms_fp64, 4),
+            "iterations_fp64": rep64["iterations"], "relres_true_fp64": rep64["relres_true"],
+            "mixed_vs_fp64_speedup": round(ms_fp64 / ms_mixed, 3),
+            "kernel_ms_mixed": rep["time_ms"], "kernel_ms_fp64": rep64["time_ms"],
+            "tile_uses": rep["tile_uses"], "nnz_uses": rep["nnz_uses"],
+            "spmv_fp64_ms": round(spmv_t, 5), "spmv_fp64_gbs": round(b_spmv / (spmv_t * 1e-3) / 1e9, 1),
+            "spmv_frac_of_hbm": round(b_spmv / (spmv_t * 1e-3) / 1e9 / peak, 3),
+            "grid": [rep["grid_blocks"], rep["threads_per_block"]], "build_ms": info["build_ms"],
+        },
+        "e2e": {"value": round(ms_e2e / world, 4), "unit": "ms", "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 3), "traffic": traffic,
+                     "kernel": "k_solve<MIXED> (persistent CG)", "peak_kind": f"{peak_kind} hbm_gbs",
+                     "algorithmic_bytes_per_launch": alg},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(A, b, rep64["iterations"], budget_s=args.cpu_budget)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def cpu_baseline(A, b, iters_to_tol, budget_s=12.0):
+    """The reference's CPU path restated (oracle FP64 tile-SpMV CG) on all host
+    threads: a bounded sample of iterations, scaled to the iteration count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    T = oracle.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+    T.cg_fp64(b, max_iter=5, fixed_iters=True, nthreads=threads)
+    done, t_total = 0, 0.0
+    while t_total < budget_s and done < 2000:
+        t0 = time.perf_counter()
+        T.cg_fp64(b, max_iter=50, fixed_iters=True, nthreads=threads)
+        t_total += time.perf_counter() - t0
+        done += 50
+    ms_it = t_total * 1e3 / done
+    return {"value": round(ms_it * iters_to_tol, 2), "unit": "ms", "cores": threads, "kind": "port",
+            "sample": f"{done} FP64 tile-SpMV CG iterations of the 128^3 system (restated reference CPU path), "
+                      f"{ms_it:.2f} ms/iteration x {iters_to_tol} iterations to 1e-8"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    A, b, _ = make_system()
+    threads = os.cpu_count() or 1
+    T = oracle.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+    t0 = time.perf_counter()
+    _, rep = T.cg_fp64(b, tol=TOL, max_iter=20000, nthreads=threads)
+    full_ms = (time.perf_counter() - t0) * 1e3
+    iters = rep["iterations"]
+    per_step = 50
+    for _ in range(args.warmup):
+        T.cg_fp64(b, max_iter=per_step, fixed_iters=True, nthreads=threads)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        T.cg_fp64(b, max_iter=per_step, fixed_iters=True, nthreads=threads)
+        ts.append((time.perf_counter() - t0) * 1e3 / per_step)
+    ms_it = statistics.mean(ts)
+    value = ms_it * iters
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_it * per_step, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD.replace("mixed-precision single-kernel CG", "FP64 CPU tile-SpMV CG"),
+                   "n": A.n, "nnz": A.nnz, "tol": TOL, "iterations_fp64_cpu": iters,
+                   "full_solve_ms": round(full_ms, 1), "relres_true": rep["relres_true"]},
+        "cpu_baseline": {"value": round(value, 2), "unit": "ms", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} x {per_step} FP64 CG iterations (oracle restatement of the "
+                                   f"reference tile loop) x {iters} iterations to 1e-8"},
+        "e2e": {"value": round(value, 2), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+        try:
+            run_ours(args, rank, world, local_rank)
+        finally:
+            dist.destroy_process_group()
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * millefeuille.h -- C ABI of the B200 (sm_100a) tile-grained mixed-precision
+ * single-kernel CG / BiCGSTAB library (libmillefeuille.so).
+ *
+ * Plain pointers and sizes only.  Two layers:
+ *
+ *  1. Drop-in entry points with the reference's exact signatures
+ *     (cg_solve_inc / cg_solve_sync / cg_solve_reduce, bicgstab /
+ *     bicgstab_sync / bicgstab_inc, Tile_create-equivalent export).
+ *  2. The native API: an opaque device-resident tiled matrix, mf_solve,
+ *     mf_spmv, tile export for parity checks, and status codes.
+ *
+ * Every function returns or records an mf_status; nothing calls exit() or
+ * traps.  Device spin-waits are bounded; a wait that runs out returns
+ * MF_ERR_TIMEOUT.  One CUDA device per process thread (the current device);
+ * handles are independent and may be used from different host threads.
+ */
+#ifndef MILLEFEUILLE_H
+#define MILLEFEUILLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum {
+    MF_SUCCESS = 0,
+    MF_ERR_INVALID = 1,        /* bad argument / malformed CSR */
+    MF_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+    MF_ERR_NOMEM = 3,          /* device allocation failed */
+    MF_ERR_TIMEOUT = 4,        /* a bounded device wait ran out */
+    MF_ERR_UNSUPPORTED = 5,    /* input outside the supported envelope */
+    MF_ERR_BREAKDOWN = 6,      /* a Krylov scalar became 0 / non-finite */
+    MF_ERR_IO = 7,             /* matrix file could not be read */
+    MF_ERR_NOT_BUILT = 8       /* no CUDA device available */
+} mf_status;
+
+const char *mf_status_string(int status);
+
+/* ------------------------------------------------------ drop-in boundary */
+
+/* Result record of the reference drivers (main-cg-mixed.cu:11-16). */
+typedef struct {
+    double time_ms;     /* solve time (CUDA events around the single launch) */
+    int iterations;     /* iterations executed */
+    double l2_norm;     /* ||A x - b|| / ||b|| computed in FP64 */
+    double residual;    /* recursive ||r|| (absolute) */
+} CgBenchResult;
+
+/*
+ * Replaces cg_solve_inc of main-cg-mixed.cu:2248 (mixed-precision single
+ * kernel).  Same arguments and meaning: n is the row count already truncated
+ * to a multiple of 16 by the caller, ori the original column count, x is
+ * zeroed and returned, exactly max_iter iterations are run (the reference has
+ * no convergence exit); iter, maxiter and threshold are ignored as in the
+ * reference; a CSV row is appended to "cg_mixed_performance.csv" unless
+ * skip_output.  Val_Low may be NULL (then (float)Val is used).
+ */
+void cg_solve_inc(int *RowPtr, int *ColIdx, double *Val, float *Val_Low, double *x, double *b,
+                  int n, int *iter, int maxiter, double threshold, char *filename, int nnzR,
+                  int ori, int max_iter, CgBenchResult *bench_result, int skip_output);
+/* Replaces cg_solve_sync of main-cg.cu:405 (FP64 single kernel). */
+void cg_solve_sync(int *RowPtr, int *ColIdx, double *Val, float *Val_Low, double *x, double *b,
+                   int n, int *iter, int maxiter, double threshold, char *filename, int nnzR,
+                   int ori, int max_iter, CgBenchResult *bench_result, int skip_output);
+/* Replaces cg_solve_reduce of main-cg.cu:19 (FP64; the reference's multi-kernel
+ * host loop becomes the same single persistent kernel here). */
+void cg_solve_reduce(int *RowPtr, int *ColIdx, double *Val, float *Val_Low, double *x, double *b,
+                     int n, int *iter, int maxiter, double threshold, char *filename, int nnzR,
+                     int ori, int max_iter, CgBenchResult *bench_result, int skip_output);
+/*
+ * Replaces bicgstab of main-bicg-mixed.cu:1355 (mixed-precision single kernel,
+ * fixed 50 iterations, rhs overwritten with the row sums A*1 as the reference
+ * does, x is the output).  Returns 0; prints "time_bicg=... ms" like the
+ * reference and appends to "bicg_mixed_performance.csv".
+ */
+int bicgstab(int *RowPtr, int *ColIdx, double *Val, double *rhs, double *x, int nnzR,
+             char *filename, int n);
+/* Replace bicgstab_sync / bicgstab_inc of main-bicg.cu:13,711 (FP64 single
+ * kernel, fixed 50 iterations, rhs overwritten with row sums). */
+int bicgstab_sync(int *RowPtr, int *ColIdx, double *Val, double *rhs, double *x, int nnzR,
+                  char *filename, int n);
+int bicgstab_inc(int *RowPtr, int *ColIdx, double *Val, double *rhs, double *x, int nnzR,
+                 char *filename, int n);
+
+/*
+ * Replaces read_Dmatrix_32 (biio2.0/src/biio.h:153-194): reads a Matrix
+ * Market (.mtx) or binary CSR (.cbd) file into 0-based CSR with the
+ * reference's ordering (file order within a row, symmetric entries mirrored).
+ * Arrays are allocated with malloc; free them with mf_free_host.
+ */
+int mf_read_matrix(const char *path, int *m, int *n, int *nnz, int **rowptr, int **colidx,
+                   double **val, int *is_symmetric);
+/* Writes binary CSR (.cbd, biio.h:74-97 layout). */
+int mf_write_cbd(const char *path, int m, int n, int nnz, const int *rowptr, const int *colidx,
+                 const double *val);
+void mf_free_host(void *p);
+
+/* ------------------------------------------------------------ native API */
+
+typedef enum { MF_METHOD_CG = 0, MF_METHOD_BICGSTAB = 1 } mf_method;
+
+typedef enum {
+    MF_PREC_FP64 = 0,     /* all tiles FP64 ("same kernel in all-FP64") */
+    MF_PREC_MIXED = 1,    /* default: FP32/FP16/INT8 tile products, FP64 dots/updates */
+    MF_PREC_PARITY = 2    /* reference label rule and tile arithmetic (not numerically safe) */
+} mf_precision;
+
+typedef struct {
+    int method;            /* mf_method */
+    int precision;         /* mf_precision */
+    double tol;            /* relative residual target ||b-Ax||/||b|| */
+    int max_iter;          /* iteration cap */
+    int fixed_iters;       /* 1: run exactly max_iter iterations (reference semantics) */
+    int replace_every;     /* FP64 true-residual replacement period (0: only at convergence) */
+    double demote_fp16;    /* mixed: column segment max|p| / max|p| below this -> FP16 tiles */
+    double demote_int8;    /* mixed: ... below this -> scaled INT8 tiles */
+    int use_lossless;      /* mixed: tiles exactly representable in a narrower type use it */
+    double wait_timeout_s; /* bound on every device spin-wait */
+    int blocks_per_sm;     /* 0: from occupancy */
+    int threads_per_block; /* 0: default (512) */
+    int x0_given;          /* 1: x holds the initial guess on entry (not supported yet) */
+    int test_stall_barrier;/* test hook: 1 = the first grid barrier waits for one arrival that
+                              never comes; the bounded wait runs out after wait_timeout_s and the
+                              solve returns MF_ERR_TIMEOUT (no fault, the context stays usable) */
+} mf_options;
+
+typedef struct {
+    int status;            /* mf_status of the solve */
+    int iterations;
+    int converged;
+    double relres_true;    /* FP64 ||b - A x|| / ||b|| at exit (on the GPU) */
+    double relres_rec;     /* recursive residual ratio at exit */
+    double residual;       /* recursive ||r|| (absolute) */
+    double time_ms;        /* kernel time (CUDA events on the launch stream) */
+    int replacements;      /* FP64 residual replacements performed */
+    int grid_blocks;       /* persistent grid size */
+    int threads_per_block;
+    long long tile_uses[4];/* tile-products executed per precision: FP64, FP32, FP16, INT8 */
+    long long tiles_skipped;
+    long long nnz_uses[4]; /* matrix entries streamed per precision (same order); the FP64
+                              residual-replacement SpMVs are not included */
+} mf_report;
+
+void mf_options_default(mf_options *opt);
+
+typedef struct mf_matrix_s *mf_matrix;
+
+typedef struct {
+    int n_rows, n_cols;
+    long long nnz;
+    int tilem, tilen, tilenum;
+    int csrsize, csrptrlen, cnt_non_new, rowblkblock;
+    int nseg;               /* solver slices */
+    long long slice_entries;/* padded solver entries */
+    double build_ms;        /* GPU tiling + encoding time */
+} mf_matrix_info;
+
+/*
+ * Build a device-resident tiled matrix from 0-based CSR (n_rows rows; rows are
+ * NOT truncated here).  Pointers are host pointers unless device_ptrs != 0.
+ * val_low may be NULL ((float)val is used).  The GPU csr2block is bit-exact to
+ * Tile_create (csr2block.h:267-422).  stream may be NULL (default stream).
+ */
+int mf_matrix_create(mf_matrix *out, int n_rows, int n_cols, long long nnz, const int *rowptr,
+                     const int *colidx, const double *val, const float *val_low, int device_ptrs,
+                     void *stream);
+int mf_matrix_destroy(mf_matrix A);
+int mf_matrix_get_info(mf_matrix A, mf_matrix_info *info);
+
+/*
+ * Copy one reference-layout array to host memory (for parity checks).  Names:
+ * tile_ptr, tile_columnidx, tile_nnz, blknnz, csr_offset, csrptr_offset,
+ * ptroffset1, ptroffset2, val, val_low, col, ptr, nonzero_row_new,
+ * blockrowid_new, blockcsr_ptr_new, tile_rowidx, block_signal,
+ * blkcoostylerowidx, colstart, colstop, val_f16, val_i8_ref, val_i8, i8_scale.
+ * bytes must equal the array size; mf_tile_array_bytes reports it.
+ */
+int mf_tile_array_bytes(mf_matrix A, const char *name, size_t *bytes);
+int mf_tile_export(mf_matrix A, const char *name, void *host_dst, size_t bytes);
+
+/*
+ * Solve A x = b (or with nrhs=1 only in this version).  b and x are host
+ * pointers unless device_ptrs != 0; with host pointers the copies are part of
+ * the call.  report may be NULL.
+ */
+int mf_solve(mf_matrix A, const double *b, double *x, const mf_options *opt, mf_report *report,
+             int device_ptrs, void *stream);
+
+/* y = A x with the tile kernel.  precision: MF_PREC_FP64 or MF_PREC_MIXED
+ * (MIXED here means every tile in FP32).  elapsed_ms (nullable) gets the kernel time. */
+int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs,
+            void *stream, double *elapsed_ms);
+
+/* Test hook: segment labels of the reference rule for (p_old, p_new) device or
+ * host arrays of length nseg*16; codes as d_vis (0 FP64, 4 FP32, 3 FP16, 2 INT8,
+ * 1 bypass).  Runs the same device classifier the parity-mode solver uses. */
+int mf_debug_ref_labels(const double *p_old, const double *p_new, int nseg, int *vis,
+                        int device_ptrs);
+
+/* Library build identity (e.g. "sm_100a"). */
+const char *mf_build_arch(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MILLEFEUILLE_H */

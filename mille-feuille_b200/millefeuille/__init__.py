@@ -1,0 +1,186 @@
+"""millefeuille -- B200 (sm_100a) tile-grained mixed-precision single-kernel
+CG / BiCGSTAB, a drop-in for Mille-feuille's solver path.
+
+Host-side mirror of the C ABI (include/millefeuille.h):
+
+    A = Matrix.from_csr(n_rows, n_cols, rowptr, colidx, val)   # GPU csr2block + encoder
+    x, rep = A.solve(b, method="cg", precision="mixed", tol=1e-8)
+    y = A.spmv(x)
+    A.export("tile_ptr")                                     # reference-layout arrays
+
+Inputs may be numpy arrays (host) or CUDA torch tensors (device, float64 /
+int32).  All compute runs in libmillefeuille.so; nothing here falls back to
+the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (MF_METHOD_BICGSTAB, MF_METHOD_CG, MF_PREC_FP64, MF_PREC_MIXED, MF_PREC_PARITY, MFError,
+                   Options, Report, check)
+
+__all__ = ["Matrix", "Options", "Report", "MFError", "default_options", "read_matrix", "write_cbd",
+           "MF_PREC_FP64", "MF_PREC_MIXED", "MF_PREC_PARITY", "MF_METHOD_CG", "MF_METHOD_BICGSTAB"]
+
+_PREC = {"fp64": MF_PREC_FP64, "mixed": MF_PREC_MIXED, "parity": MF_PREC_PARITY}
+_METHOD = {"cg": MF_METHOD_CG, "bicgstab": MF_METHOD_BICGSTAB}
+
+# dtype of every reference-layout array mf_tile_export can return
+EXPORT_DTYPES = {
+    "tile_ptr": np.int32, "tile_columnidx": np.int32, "tile_nnz": np.int32, "blknnz": np.int32,
+    "csr_offset": np.int32, "csrptr_offset": np.int32, "ptroffset1": np.int32, "ptroffset2": np.int32,
+    "val": np.float64, "val_low": np.float32, "col": np.uint8, "ptr": np.uint8,
+    "nonzero_row_new": np.int32, "blockrowid_new": np.uint8, "blockcsr_ptr_new": np.uint8,
+    "tile_rowidx": np.int32, "block_signal": np.int32, "blkcoostylerowidx": np.uint32,
+    "colstart": np.int32, "colstop": np.int32, "val_f16": np.uint16, "val_i8_ref": np.int8,
+    "val_i8": np.int8, "i8_scale": np.float32, "tile_caps": np.uint8, "seg_ptr": np.int32,
+    "seg_kp": np.int32, "seg_rowlen": np.uint16, "seg_off": np.int64, "meta": np.uint8, "v64": np.float64,
+}
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    _lib.load().mf_options_default(C.byref(o))
+    for k, v in kw.items():
+        if k == "precision" and isinstance(v, str):
+            v = _PREC[v]
+        if k == "method" and isinstance(v, str):
+            v = _METHOD[v]
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+def _is_cuda_tensor(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if _is_cuda_tensor(a):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Matrix:
+    """Device-resident tiled matrix (an mf_matrix handle)."""
+
+    def __init__(self, handle, keep=None):
+        self._h = handle
+        self._keep = keep
+
+    @classmethod
+    def from_csr(cls, n_rows, n_cols, rowptr, colidx, val, val_low=None, stream=None) -> "Matrix":
+        L = _lib.load()
+        dev = _is_cuda_tensor(rowptr)
+        if not dev:
+            rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+            colidx = np.ascontiguousarray(colidx, dtype=np.int32)
+            val = np.ascontiguousarray(val, dtype=np.float64)
+            if val_low is not None:
+                val_low = np.ascontiguousarray(val_low, dtype=np.float32)
+        nnz = int(colidx.numel() if dev else colidx.size)
+        h = C.c_void_p()
+        check(L.mf_matrix_create(C.byref(h), int(n_rows), int(n_cols), nnz, _ptr(rowptr), _ptr(colidx), _ptr(val),
+                                 _ptr(val_low), int(dev), C.c_void_p(stream) if stream else None),
+              "mf_matrix_create")
+        return cls(h)
+
+    def close(self) -> None:
+        if self._h:
+            _lib.load().mf_matrix_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def info(self) -> dict:
+        inf = _lib.MatrixInfo()
+        check(_lib.load().mf_matrix_get_info(self._h, C.byref(inf)), "mf_matrix_get_info")
+        return {k: getattr(inf, k) for k, _ in inf._fields_}
+
+    def export(self, name: str) -> np.ndarray:
+        L = _lib.load()
+        nb = C.c_size_t()
+        check(L.mf_tile_array_bytes(self._h, name.encode(), C.byref(nb)), f"mf_tile_array_bytes({name})")
+        dt = np.dtype(EXPORT_DTYPES[name])
+        out = np.zeros(nb.value // dt.itemsize, dtype=dt)
+        check(L.mf_tile_export(self._h, name.encode(), out.ctypes.data_as(C.c_void_p), nb.value),
+              f"mf_tile_export({name})")
+        return out
+
+    def solve(self, b, x=None, options: Options | None = None, stream=None, **kw):
+        """Solve A x = b.  b: numpy float64 (host) or CUDA float64 tensor
+        (device).  Returns (x, report dict); raises MFError on failure
+        (the report is attached as err.report)."""
+        L = _lib.load()
+        o = options if options is not None else default_options(**kw)
+        if options is not None and kw:
+            for k, v in kw.items():
+                setattr(o, k, _PREC.get(v, v) if k == "precision" else _METHOD.get(v, v) if k == "method" else v)
+        dev = _is_cuda_tensor(b)
+        if x is None:
+            if dev:
+                import torch
+                x = torch.zeros_like(b)
+            else:
+                b = np.ascontiguousarray(b, dtype=np.float64)
+                x = np.zeros_like(b)
+        rep = Report()
+        st = L.mf_solve(self._h, _ptr(b), _ptr(x), C.byref(o), C.byref(rep), int(dev),
+                        C.c_void_p(stream) if stream else None)
+        if st != _lib.MF_SUCCESS:
+            err = MFError(st, "mf_solve")
+            err.report = rep.as_dict()
+            raise err
+        return x, rep.as_dict()
+
+    def spmv(self, x, y=None, precision="fp64", stream=None):
+        L = _lib.load()
+        dev = _is_cuda_tensor(x)
+        n_rows = self.info["n_rows"]
+        if y is None:
+            if dev:
+                import torch
+                y = torch.empty(n_rows, dtype=torch.float64, device=x.device)
+            else:
+                x = np.ascontiguousarray(x, dtype=np.float64)
+                y = np.zeros(n_rows, dtype=np.float64)
+        ms = C.c_double()
+        check(L.mf_spmv(self._h, _ptr(x), _ptr(y), _PREC[precision] if isinstance(precision, str) else precision,
+                        int(dev), C.c_void_p(stream) if stream else None, C.byref(ms)), "mf_spmv")
+        self.last_spmv_ms = ms.value
+        return y
+
+
+def read_matrix(path: str):
+    """Reads .mtx / .cbd with the reference's semantics; returns
+    (m, n, rowptr, colidx, val, is_symmetric) as numpy arrays."""
+    L = _lib.load()
+    m, n, nnz, sym = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    rp, ci, vv = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()
+    check(L.mf_read_matrix(path.encode(), C.byref(m), C.byref(n), C.byref(nnz), C.byref(rp), C.byref(ci),
+                           C.byref(vv), C.byref(sym)), f"mf_read_matrix({path})")
+    rowptr = np.ctypeslib.as_array(rp, shape=(m.value + 1,)).copy()
+    colidx = np.ctypeslib.as_array(ci, shape=(max(nnz.value, 1),))[: nnz.value].copy()
+    val = np.ctypeslib.as_array(vv, shape=(max(nnz.value, 1),))[: nnz.value].copy()
+    for p in (rp, ci, vv):
+        L.mf_free_host(C.cast(p, C.c_void_p))
+    return m.value, n.value, rowptr, colidx, val, bool(sym.value)
+
+
+def write_cbd(path: str, m: int, n: int, rowptr, colidx, val) -> None:
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+    colidx = np.ascontiguousarray(colidx, dtype=np.int32)
+    val = np.ascontiguousarray(val, dtype=np.float64)
+    check(_lib.load().mf_write_cbd(path.encode(), int(m), int(n), int(colidx.size), _ptr(rowptr), _ptr(colidx),
+                                   _ptr(val)), "mf_write_cbd")

@@ -1,0 +1,103 @@
+"""CPU tests of the C ABI: the library loads, exports every symbol the header
+declares, and its host-only entry points (status strings, options, matrix
+reader / writer) behave; no compute call is made without a GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
+
+
+def _declared_functions():
+    names = set()
+    for h in HEADERS:
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?[\s\*])([A-Za-z_]\w*)\s*\(", src, flags=re.M):
+            name = m.group(1)
+            if name not in ("if", "while", "for", "return", "sizeof", "defined"):
+                names.add(name)
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(mf):
+    from millefeuille import _lib
+    L = _lib.load()
+    declared = _declared_functions()
+    assert len(declared) >= 20
+    missing = [n for n in declared if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(_lib.EXPORTED) <= set(declared)
+
+
+def test_status_strings_and_defaults(mf):
+    from millefeuille import _lib
+    L = _lib.load()
+    assert L.mf_build_arch().decode() == "sm_100a"
+    for s in range(0, 9):
+        assert len(_lib.status_string(s)) > 3
+    o = mf.default_options()
+    assert o.precision == mf.MF_PREC_MIXED and o.replace_every == 50 and o.tol == 1e-8
+    o2 = mf.default_options(precision="fp64", method="bicgstab", tol=1e-10)
+    assert o2.precision == 0 and o2.method == 1 and o2.tol == 1e-10
+
+
+def test_no_device_reports_not_built(mf):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(mf.MFError) as e:
+        mf.Matrix.from_csr(2, 2, np.array([0, 1, 2]), np.array([0, 1]), np.array([1.0, 1.0]))
+    assert e.value.status == 8
+
+
+@pytest.mark.parametrize("field,sym", [("real", False), ("real", True), ("pattern", False), ("integer", True)])
+def test_mtx_reader_matches_oracle_and_reference(mf, oracle_mod, tmp_path, field, sym):
+    from millefeuille import matrices as M
+    A = M.random_csr(70, 70, 0.08, seed=5)
+    S = A.to_scipy()
+    if sym:
+        S = (S + S.T).tocsr()
+        S.sort_indices()
+        A = M.CSR(70, S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data * 3.0)
+    if field == "integer":
+        A.val = np.round(A.val * 10)
+    path = str(tmp_path / "m.mtx")
+    M.write_mtx(path, A, symmetric=sym, field=field)
+    got = mf.read_matrix(path)
+    exp = oracle_mod.read_mtx(path)
+    for g, e in zip(got[2:5], exp[2:5]):
+        np.testing.assert_array_equal(g, e)
+    assert got[:2] == exp[:2] and got[5] == exp[5]
+    if oracle_mod.ref_available():
+        ref = oracle_mod.ref_read_matrix(path)
+        for g, e in zip(got[2:5], ref[2:5]):
+            np.testing.assert_array_equal(g, e)
+
+
+def test_cbd_roundtrip(mf, tmp_path):
+    from millefeuille import matrices as M
+    A = M.random_csr(50, 60, 0.1, seed=6)
+    p = str(tmp_path / "a.cbd")
+    mf.write_cbd(p, 50, 60, A.rowptr, A.colidx, A.val)
+    m, n, rp, ci, vv, sym = mf.read_matrix(p)
+    assert (m, n) == (50, 60)
+    np.testing.assert_array_equal(rp, A.rowptr)
+    np.testing.assert_array_equal(ci, A.colidx)
+    np.testing.assert_array_equal(vv, A.val)
+    p2 = str(tmp_path / "b.cbd")
+    M.write_cbd(p2, A, ncols=60)
+    assert open(p, "rb").read() == open(p2, "rb").read()
+
+
+def test_reader_rejects_bad_files(mf, tmp_path):
+    p = tmp_path / "bad.mtx"
+    p.write_text("%%MatrixMarket matrix array real general\n2 2\n1\n2\n3\n4\n")
+    with pytest.raises(mf.MFError):
+        mf.read_matrix(str(p))
+    with pytest.raises(mf.MFError):
+        mf.read_matrix(str(tmp_path / "missing.mtx"))

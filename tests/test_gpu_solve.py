@@ -1,0 +1,180 @@
+"""GPU parity of the tile SpMV and the persistent CG / BiCGSTAB kernel against
+the FP64 oracle (the reference's algorithm restated on the CPU).
+
+Tolerances: SpMV FP64 rtol 1e-13 (summation order differs from the oracle's);
+FP32 tiles rtol 1e-5; solver iteration counts within 5 % (+1) of the oracle's;
+every converged solve is checked with an independent FP64 residual."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _relres(A, x, b):
+    return np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def lap64():
+    from millefeuille import matrices as M
+    return M.laplace2d_system(64, seed=0)
+
+
+@pytest.fixture(scope="module")
+def p3d():
+    from millefeuille import matrices as M
+    return M.poisson3d_varcoef(32, seed=1)
+
+
+@pytest.fixture(scope="module")
+def cd3d():
+    from millefeuille import matrices as M
+    return M.convdiff3d(20, seed=2)
+
+
+def test_gpu_spmv_fp64_and_fp32(mf, cuda):
+    from millefeuille import matrices as M
+    for A in (M.laplace2d(64), M.poisson3d_varcoef(24, seed=1)[0], M.random_csr(500, 530, 0.03, seed=2)):
+        ncols = int(A.colidx.max()) + 1 if A.nnz else A.n
+        ncols = max(ncols, A.n)
+        G = mf.Matrix.from_csr(A.n, ncols, A.rowptr, A.colidx, A.val)
+        x = np.random.default_rng(0).standard_normal(ncols)
+        S = A.to_scipy() if ncols == A.n else __import__("scipy.sparse", fromlist=["csr_matrix"]).csr_matrix(
+            (A.val, A.colidx, A.rowptr), shape=(A.n, ncols))
+        y_ref = S @ x
+        y = G.spmv(x, precision="fp64")
+        np.testing.assert_allclose(y, y_ref, rtol=1e-13, atol=1e-13 * np.abs(y_ref).max())
+        y32 = G.spmv(x, precision="mixed")
+        np.testing.assert_allclose(y32, y_ref, rtol=1e-5, atol=1e-5 * np.abs(y_ref).max())
+
+
+def test_gpu_cg_fp64_matches_oracle(mf, oracle_mod, cuda, lap64):
+    A, b, xt = lap64
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x, rep = G.solve(b, method="cg", precision="fp64", tol=1e-10, replace_every=0)
+    T = oracle_mod.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+    xo, ro = T.cg_fp64(b, tol=1e-10, max_iter=10000)
+    assert rep["converged"] and rep["relres_true"] <= 1e-10
+    assert abs(rep["iterations"] - ro["iterations"]) <= 1 + 0.05 * ro["iterations"]
+    assert _relres(A, x, b) <= 1e-10
+    np.testing.assert_allclose(x, xo, rtol=0, atol=1e-7)
+    assert np.abs(x - xt).max() < 1e-6
+
+
+def test_gpu_cg_fp64_fixed_iterations_track_oracle(mf, oracle_mod, cuda, p3d):
+    A, b, _ = p3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    T = oracle_mod.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+    # FP64 CG iterates of this system are rounding-sensitive: two summation
+    # orders stay within 1e-13 for ~15 iterations, then drift apart (2e-7 at 30).
+    for k in (1, 7, 15):
+        x, rep = G.solve(b, precision="fp64", max_iter=k, fixed_iters=1, replace_every=0)
+        xo, ro = T.cg_fp64(b, max_iter=k, fixed_iters=True)
+        assert rep["iterations"] == k
+        np.testing.assert_allclose(x, xo, rtol=1e-9, atol=1e-11 * np.abs(xo).max())
+        assert rep["relres_true"] == pytest.approx(ro["relres_true"], rel=1e-6)
+
+
+def test_gpu_cg_mixed_converges_fp64_verified(mf, oracle_mod, cuda, p3d):
+    A, b, xt = p3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x, rep = G.solve(b, method="cg", precision="mixed", tol=1e-8)
+    assert rep["converged"] and rep["relres_true"] <= 1e-8
+    assert _relres(A, x, b) <= 1.0001e-8
+    T = oracle_mod.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+    _, ro = T.cg_fp64(b, tol=1e-8, max_iter=10000)
+    assert rep["iterations"] <= 1.3 * ro["iterations"] + 5
+    assert sum(rep["tile_uses"][1:]) > 0          # low-precision tiles were used
+
+
+def test_gpu_cg_deterministic(mf, cuda, p3d):
+    A, b, _ = p3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x1, r1 = G.solve(b, precision="mixed", tol=1e-8)
+    x2, r2 = G.solve(b, precision="mixed", tol=1e-8)
+    assert r1["iterations"] == r2["iterations"]
+    np.testing.assert_array_equal(x1, x2)
+
+
+def test_gpu_bicgstab_fp64_matches_oracle(mf, oracle_mod, cuda, cd3d):
+    A, b, _ = cd3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x, rep = G.solve(b, method="bicgstab", precision="fp64", tol=1e-8, replace_every=0)
+    T = oracle_mod.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+    xo, ro = T.bicgstab_fp64(b, tol=1e-8, max_iter=10000)
+    assert rep["converged"] and rep["relres_true"] <= 1e-8
+    assert abs(rep["iterations"] - ro["iterations"]) <= 2 + 0.05 * ro["iterations"]
+    assert _relres(A, x, b) <= 1.0001e-8
+
+
+def test_gpu_bicgstab_mixed_converges(mf, cuda, cd3d):
+    A, b, _ = cd3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x, rep = G.solve(b, method="bicgstab", precision="mixed", tol=1e-8)
+    assert rep["converged"] and rep["relres_true"] <= 1e-8
+    assert _relres(A, x, b) <= 1.0001e-8
+
+
+def test_gpu_solve_device_pointers(mf, cuda, p3d):
+    import torch
+    A, b, _ = p3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    bd = torch.from_numpy(b).to(cuda)
+    xd, rep = G.solve(bd, precision="fp64", tol=1e-9)
+    xh, rep2 = G.solve(b, precision="fp64", tol=1e-9)
+    np.testing.assert_array_equal(xd.cpu().numpy(), xh)
+
+
+def test_gpu_barrier_timeout_is_reported_and_context_survives(mf, cuda, lap64):
+    A, b, _ = lap64
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    with pytest.raises(mf.MFError) as e:
+        G.solve(b, precision="fp64", tol=1e-8, test_stall_barrier=1, wait_timeout_s=0.2)
+    assert e.value.status == 4          # MF_ERR_TIMEOUT
+    x, rep = G.solve(b, precision="fp64", tol=1e-8)
+    assert rep["converged"]
+
+
+def test_gpu_dropin_cg_solve_entry_points(mf, oracle_mod, cuda, p3d, tmp_path, monkeypatch):
+    """cg_solve_sync / cg_solve_inc with the reference's argument list: exactly
+    max_iter iterations, x returned, l2_norm = ||Ax-b||/||b|| in FP64."""
+    from millefeuille import _lib
+    monkeypatch.chdir(tmp_path)
+    A, b, _ = p3d
+    L = _lib.load()
+    rp = A.rowptr.astype(np.int32).copy()
+    ci = A.colidx.astype(np.int32).copy()
+    vv = A.val.copy()
+    vl = vv.astype(np.float32)
+    T = oracle_mod.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+    for name, prec in (("cg_solve_sync", "fp64"), ("cg_solve_inc", "mixed")):
+        x = np.ones(A.n)
+        res = _lib.CgBenchResult()
+        it = C.c_int(0)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        getattr(L, name)(ip(rp), ip(ci), dp(vv), vl.ctypes.data_as(C.POINTER(C.c_float)), dp(x), dp(b.copy()),
+                         A.n, C.byref(it), 10, 1e-5, b"p3d", A.nnz, A.n, 12, C.byref(res), 0)
+        assert res.iterations == 12
+        assert res.l2_norm == pytest.approx(_relres(A, x, b), rel=1e-6)
+        if prec == "fp64":
+            _, ro = T.cg_fp64(b, max_iter=12, fixed_iters=True)
+            assert res.l2_norm == pytest.approx(ro["relres_true"], rel=1e-6)
+    assert (tmp_path / "cg_performance.csv").exists() and (tmp_path / "cg_mixed_performance.csv").exists()
+
+
+def test_gpu_dropin_bicgstab(mf, cuda, cd3d, tmp_path, monkeypatch):
+    from millefeuille import _lib
+    monkeypatch.chdir(tmp_path)
+    A, _, _ = cd3d
+    L = _lib.load()
+    rhs = np.zeros(A.n)
+    x = np.zeros(A.n)
+    rc = L.bicgstab_sync(A.rowptr.ctypes.data_as(C.POINTER(C.c_int)), A.colidx.ctypes.data_as(C.POINTER(C.c_int)),
+                         A.val.ctypes.data_as(C.POINTER(C.c_double)), rhs.ctypes.data_as(C.POINTER(C.c_double)),
+                         x.ctypes.data_as(C.POINTER(C.c_double)), A.nnz, b"cd", A.n)
+    assert rc == 0
+    np.testing.assert_allclose(rhs, A.to_scipy() @ np.ones(A.n), rtol=1e-14)
+    assert _relres(A, x, rhs) < 1e-6          # 50 fixed iterations on a well-conditioned system
