@@ -300,8 +300,42 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def run_profile(args):
+    """Small fixed-size launches for ncu: build the 128^3 system, run the chosen
+    kernel once to warm up, then once more (the launch to capture), and exit."""
+    import numpy as np
+    import torch
+    import millefeuille as mf
+    dev = torch.device("cuda", 0)
+    A, b, _ = make_system()
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    bd = torch.from_numpy(b).to(dev)
+    xd = torch.zeros_like(bd)
+    kind = args.profile
+    if kind.startswith("spmv"):
+        prec = "fp64" if kind == "spmv_fp64" else "mixed"
+        xs = torch.from_numpy(np.random.default_rng(7).uniform(-1, 1, A.n)).to(dev)
+        ys = torch.empty_like(xs)
+        for _ in range(2):
+            G.spmv(xs, ys, precision=prec)
+        print(json.dumps({"profile": kind, "spmv_ms": G.last_spmv_ms}))
+        return
+    prec = "fp64" if kind == "solve_fp64" else "mixed"
+    o = mf.default_options(precision=prec, tol=TOL, max_iter=args.profile_iters, fixed_iters=1, replace_every=0,
+                           blocks_per_sm=args.blocks_per_sm)
+    for _ in range(2):
+        _, rep = G.solve(bd, xd, options=o)
+    print(json.dumps({"profile": kind, "iterations": rep["iterations"], "kernel_ms": rep["time_ms"],
+                      "grid": [rep["grid_blocks"], rep["threads_per_block"]], "nnz_uses": rep["nnz_uses"],
+                      "tile_uses": rep["tile_uses"]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile", choices=["solve_fp64", "solve_mixed", "spmv_fp64", "spmv_mixed"],
+                    help="run one small launch of a kernel for an ncu capture and exit")
+    ap.add_argument("--profile-iters", type=int, default=20)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -309,6 +343,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

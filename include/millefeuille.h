@@ -123,6 +123,8 @@ typedef struct {
     int blocks_per_sm;     /* 0: from occupancy */
     int threads_per_block; /* 0: default (512) */
     int x0_given;          /* 1: x holds the initial guess on entry (not supported yet) */
+    int l2_window;         /* 1 (default): keep the solver vectors in L2 with a persisting
+                              access-policy window on the stream during the solve */
     int test_stall_barrier;/* test hook: 1 = the first grid barrier waits for one arrival that
                               never comes; the bounded wait runs out after wait_timeout_s and the
                               solve returns MF_ERR_TIMEOUT (no fault, the context stays usable) */
@@ -143,6 +145,9 @@ typedef struct {
     long long tiles_skipped;
     long long nnz_uses[4]; /* matrix entries streamed per precision (same order); the FP64
                               residual-replacement SpMVs are not included */
+    double phase_ms[6];    /* block 0's wall time split: SpMV phases, first vector update,
+                              direction update, barriers + reductions, FP64 residual replacement;
+                              [5]: of the barrier time, block 0 spinning for the other blocks */
 } mf_report;
 
 void mf_options_default(mf_options *opt);

@@ -60,6 +60,8 @@ void mf_options_default(mf_options *o)
     o->blocks_per_sm = 0;
     o->threads_per_block = 0;
     o->x0_given = 0;
+    o->l2_window = 1;
+    o->test_stall_barrier = 0;
 }
 
 void mf_free_host(void *p) { free(p); }
@@ -85,8 +87,8 @@ void free_matrix(mf_matrix_s *A)
                     A->d_nonzero_row_new, A->d_tile_rowidx, A->d_block_signal, A->d_blockrowid_new,
                     A->d_blockcsr_ptr_new, A->d_rb_idx, A->d_rb_start, A->d_rb_stop, A->d_val_f16,
                     A->d_val_i8_ref, A->d_val_i8, A->d_i8_scale, A->d_tile_caps, A->d_seg_ptr, A->d_seg_tile0,
-                    A->d_seg_off, A->d_seg_kp, A->d_seg_rowlen, A->d_meta, A->d_v64, A->d_v32, A->d_v16,
-                    A->d_v8, A->d_row_cost};
+                    A->d_seg_off, A->d_seg_hdr, A->d_seg_kp, A->d_seg_rowlen, A->d_meta, A->d_v64, A->d_v32, A->d_v16,
+                    A->d_v8, A->d_v8ref, A->d_row_cost};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     delete A;
@@ -214,6 +216,8 @@ ArrayRef lookup(mf_matrix_s *A, const char *name)
     if (s == "seg_off") return {A->d_seg_off, ((size_t)A->nseg + 1) * 8};
     if (s == "meta") return {A->d_meta, (size_t)A->slice_entries};
     if (s == "v64") return {A->d_v64, (size_t)A->slice_entries * 8};
+    if (s == "v32") return {A->d_v32, (size_t)A->slice_entries * 4};
+    if (s == "seg_hdr") return {A->d_seg_hdr, (size_t)A->nseg * 16};
     return {nullptr, 0};
 }
 }  // namespace

@@ -70,6 +70,7 @@ struct mf_matrix_s {
     int *d_seg_ptr;            // [tilem+1]
     int *d_seg_tile0;          // [nseg+1] first tile of each segment (+ end)
     long long *d_seg_off;      // [nseg+1] entry offset
+    int4 *d_seg_hdr;           // [nseg+1] {first tile, tile-row, kp | ntiles << 16 | last << 24, offset / 128}
     int *d_seg_kp;             // [nseg]
     uint16_t *d_seg_rowlen;    // [nseg*16]
     long long slice_entries;
@@ -78,6 +79,7 @@ struct mf_matrix_s {
     float *d_v32;
     __half *d_v16;
     int8_t *d_v8;
+    int8_t *d_v8ref;           // reference (unscaled, truncated) int8 values, parity mode only
     // tile-row ownership cost prefix for partitioning: [tilem+1]
     long long *d_row_cost;
     double build_ms;

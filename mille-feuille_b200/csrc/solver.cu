@@ -7,11 +7,15 @@
 //  * a half-warp owns a contiguous range of tile-rows (lane i = row 16R+i) for
 //    every phase, so y rows are written by their owner only (no y atomics) and
 //    every dot product is reduced in a fixed order (deterministic);
+//  * the tile SpMV walks the half-warp's solver slices as a software pipeline:
+//    one 16-byte header per slice, the slice's tile table held one tile per
+//    lane (read with __shfl_sync), the next slice's header / tiles / index bytes
+//    prefetched while the current slice's eight value + x loads are in flight;
 //  * the grid barrier is a monotone counter: red.release.gpu arrive, polled with
 //    ld.acquire.gpu, every wait bounded by %globaltimer (MF_ERR_TIMEOUT);
 //  * dot products: warp shuffle tree -> per-block partial in a fixed slot ->
 //    after the barrier each block sums the partials in the same order;
-//  * matrix payload is streamed with evict-first loads; vectors stay L2-friendly.
+//  * matrix payload is streamed with evict-first loads so the vectors stay in L2.
 #include "mf_internal.cuh"
 
 #include <cmath>
@@ -22,21 +26,22 @@ namespace {
 
 constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
-constexpr int kRedKinds = 8;      // reduction slot groups
+constexpr int kRedKinds = 10;     // reduction slot groups
 constexpr int kRedWidth = 4;      // doubles per group per block
+constexpr int kDefaultLB = 2;     // default register-budget variant of the persistent kernel
 
 enum { MODE_FP64 = 0, MODE_MIXED = 1, MODE_PARITY = 2 };
 
 struct SolverParams {
     int n, tilem, vec_len;
-    const int *seg_ptr, *seg_tile0, *seg_kp;
-    const long long *seg_off;
+    const int *seg_ptr;
+    const int4 *seg_hdr;
     const uint16_t *seg_rowlen;
     const unsigned char *meta;
     const double *v64;
     const float *v32;
     const __half *v16;
-    const int8_t *v8;
+    const int8_t *v8, *v8ref;
     const int *tile_col;
     const int *tile_off;          // csr_offset: tile payload offsets (tile nnz for the counters)
     const float *i8_scale;
@@ -45,12 +50,15 @@ struct SolverParams {
     const double *b;
     double *x, *r, *p, *q, *rh, *s, *t;
     float *p32, *s32, *mag_p, *mag_s;
+    __half *p16, *s16;
+    int8_t *p8, *s8;
     signed char *lab_p, *lab_s;
     double *red;
     unsigned int *bar;
     int *err;
     double *out;
     unsigned long long *counts;
+    unsigned long long *phase_ns;   // [8] block-0 time per phase: spmv, vecB, vecC, barrier, replacement
     int method, max_iter, fixed_iters, replace_every, use_lossless;
     double tol;
     float demote16, demote8;
@@ -59,12 +67,11 @@ struct SolverParams {
 };
 
 struct Shared {
-    int xb[kWarps * 32];
-    float sc[kWarps * 32];
-    signed char pr[kWarps * 32];
     double wred[kWarps][kRedWidth];
     double bcast[kRedWidth];
     int flag;
+    unsigned cnt[kWarps][10];   // per-warp tile / entry counters (tile products per precision)
+    unsigned long long clk_t, clk_acc[5];   // block 0 phase clock
 };
 
 // ------------------------------------------------------------ grid barrier
@@ -73,6 +80,7 @@ __device__ bool grid_barrier(const SolverParams &P, unsigned &epoch, Shared &sh)
     __syncthreads();
     epoch += 1;
     if (threadIdx.x == 0) {
+        const unsigned long long tw0 = mf_globaltimer();
         const unsigned target = epoch * gridDim.x + ((P.stall_first_barrier && epoch == 1) ? 1u : 0u);
         __threadfence();
         mf_red_release_add_u32(P.bar, 1u);
@@ -91,6 +99,7 @@ __device__ bool grid_barrier(const SolverParams &P, unsigned &epoch, Shared &sh)
         }
         __threadfence();
         sh.flag = ok ? 1 : 0;
+        if (blockIdx.x == 0 && P.phase_ns) P.phase_ns[5] += mf_globaltimer() - tw0;   // block 0 spin time
     }
     __syncthreads();
     return sh.flag != 0;
@@ -156,118 +165,236 @@ __device__ void grid_collect(const SolverParams &P, Shared &sh, int kind, int nv
     __syncthreads();
 }
 
-// ------------------------------------------------------------ tile SpMV row
+// ------------------------------------------------------------ tile SpMV
 // Reference-rule label code (d_vis) -> entry precision.
 __device__ __forceinline__ int parity_prec(int code)
 {
     return code == 0 ? MF_P64 : code == 4 ? MF_P32 : code == 3 ? MF_P16 : code == 2 ? MF_P8 : MF_PSKIP;
 }
 
-// y for row 16R+i of the half-warp's tile-row R.  force_pr >= 0 forces one
-// precision for every tile (used by the FP64 residual replacement and SpMV).
-template <int MODE>
-__device__ __forceinline__ double spmv_row(const SolverParams &P, Shared &sh, int R, int i, int tb, unsigned hmask,
-                                           const double *x64, const float *x32, const float *mag, float invM,
-                                           const signed char *lab, int force_pr, unsigned long long *cnt)
+// The x operands of one SpMV: FP64 vector, its FP32 shadow, and (parity mode)
+// its FP16 / INT8 shadows; mag / lab are the per-column-segment statistics the
+// precision choice reads.
+struct XVec {
+    const double *x64;
+    const float *x32;
+    const __half *x16;
+    const int8_t *x8;
+    const float *mag;
+    const signed char *lab;
+    float invM;
+    int force_pr;            // >= 0: every tile in this precision
+};
+
+// Tile table of a slice, one tile per lane (lane i holds slot i).
+struct TileReg {
+    int xb;       // column-tile * 16
+    int pr;       // entry precision
+    float sc;     // int8 scale
+};
+
+__device__ __forceinline__ int hdr_kp(int4 h) { return h.z & 0xFFFF; }
+__device__ __forceinline__ int hdr_nt(int4 h) { return (h.z >> 16) & 0xFF; }
+__device__ __forceinline__ bool hdr_last(int4 h) { return (h.z >> 24) & 1; }
+__device__ __forceinline__ long long hdr_off(int4 h) { return (long long)h.w << 7; }
+
+template <int MODE, bool F64>
+__device__ __forceinline__ TileReg load_tiles(const SolverParams &P, int4 h, int i, const XVec &X,
+                                              unsigned *cnt)
 {
+    TileReg T;
+    T.xb = 0;
+    T.pr = MF_P64;
+    T.sc = 0.0f;
+    const int nt = hdr_nt(h);
+    if (i < nt) {
+        const int t = h.x + i;
+        const int jc = P.tile_col[t];
+        T.xb = jc * MF_BS;
+        int pr;
+        if (F64 || MODE == MODE_FP64) {
+            pr = MF_P64;
+        } else if (X.force_pr >= 0) {
+            pr = X.force_pr;
+        } else if (MODE == MODE_MIXED) {
+            const unsigned cap = P.tile_caps[t];
+            const float rel = X.mag[jc] * X.invM;
+            pr = MF_P32;
+            if (rel <= P.demote8) pr = MF_P8;
+            else if (rel <= P.demote16 && (cap & MF_CAP_FP16_OK)) pr = MF_P16;
+            if (P.use_lossless) {
+                if (cap & MF_CAP_EXACT_I8) pr = MF_P8;
+                else if ((cap & MF_CAP_EXACT_F16) && pr == MF_P32) pr = MF_P16;
+            }
+            if (pr == MF_P8) T.sc = P.i8_scale[t];
+        } else {
+            pr = parity_prec(X.lab[jc]);
+        }
+        T.pr = pr;
+        if (cnt) {
+            // shared per-warp counters; a warp's counts stay far below 2^32 per solve
+            atomicAdd(&cnt[pr], 1u);                                            // tile products
+            atomicAdd(&cnt[5 + pr], (unsigned)(P.tile_off[t + 1] - P.tile_off[t]));  // entries
+        }
+    }
+    return T;
+}
+
+// Uniform-precision chunk loop: every entry of the slice uses precision PR
+// (FP64 values with FP64 x; otherwise FP32 x, FP32 products and an FP32
+// partial sum per 8-entry chunk, added to the FP64 row sum).
+template <int PR>
+__device__ __forceinline__ double slice_dot_uniform(const SolverParams &P, long long off, int kp, int i,
+                                                    unsigned hmask, int len, const TileReg &T, const XVec &X)
+{
+    const unsigned long long *mrow = (const unsigned long long *)(P.meta + off + (long long)i * kp);
     double acc = 0.0;
-    const int s_beg = P.seg_ptr[R], s_end = P.seg_ptr[R + 1];
-    for (int s = s_beg; s < s_end; s++) {
-        const int t0 = P.seg_tile0[s];
-        const int nt = P.seg_tile0[s + 1] - t0 < MF_SEG_TILES ? P.seg_tile0[s + 1] - t0 : MF_SEG_TILES;
-        if (i < nt) {
-            const int t = t0 + i;
-            const int jc = P.tile_col[t];
-            int pr;
-            if (force_pr >= 0 || MODE == MODE_FP64) {
-                pr = force_pr >= 0 ? force_pr : MF_P64;
-            } else if (MODE == MODE_MIXED) {
-                const unsigned cap = P.tile_caps[t];
-                const float rel = mag[jc] * invM;
-                pr = MF_P32;
-                if (rel <= P.demote8) pr = MF_P8;
-                else if (rel <= P.demote16 && (cap & MF_CAP_FP16_OK)) pr = MF_P16;
-                if (P.use_lossless) {
-                    if (cap & MF_CAP_EXACT_I8) pr = MF_P8;
-                    else if ((cap & MF_CAP_EXACT_F16) && pr == MF_P32) pr = MF_P16;
-                }
-            } else {
-                pr = parity_prec(lab[jc]);
-            }
-            sh.xb[tb + i] = jc * MF_BS;
-            sh.pr[tb + i] = (signed char)pr;
-            sh.sc[tb + i] = P.i8_scale[t];
-            if (cnt) {
-                const unsigned long long nz = (unsigned long long)(P.tile_off[t + 1] - P.tile_off[t]);
+    for (int k0 = 0; k0 < kp; k0 += 8) {
+        const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
+        if (PR == MF_P64) {
+            double v[8], xv[8];
 #pragma unroll
-                for (int j = 0; j < 5; j++) {
-                    cnt[j] += (pr == j) ? 1ull : 0ull;       // tile products per precision
-                    cnt[5 + j] += (pr == j) ? nz : 0ull;     // entries per precision
-                }
+            for (int j = 0; j < 8; j++) {
+                const int k = k0 + j;
+                const bool act = k < len;
+                const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+                const int xi = __shfl_sync(hmask, T.xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
+                const long long e = off + (long long)k * MF_BS + i;
+                v[j] = act ? __ldcs(P.v64 + e) : 0.0;
+                xv[j] = act ? X.x64[xi] : 0.0;
             }
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc = fma(v[j], xv[j], acc);
+        } else {
+            float v[8], xv[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int k = k0 + j;
+                const bool act = k < len;
+                const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+                const int slot = (int)(mm >> 4);
+                const int xi = __shfl_sync(hmask, T.xb, slot, 16) + (int)(mm & 15u);
+                const long long e = off + (long long)k * MF_BS + i;
+                float fv;
+                if (PR == MF_P32) fv = act ? __ldcs(P.v32 + e) : 0.0f;
+                else if (PR == MF_P16) fv = act ? __half2float(P.v16[e]) : 0.0f;
+                else fv = act ? (float)P.v8[e] * __shfl_sync(hmask, T.sc, slot, 16) : 0.0f;
+                v[j] = fv;
+                xv[j] = act ? X.x32[xi] : 0.0f;
+            }
+            float part = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 8; j++) part = fmaf(v[j], xv[j], part);
+            acc += (double)part;
         }
-        __syncwarp(hmask);
-        const long long off = P.seg_off[s];
-        const int kp = P.seg_kp[s];
-        const int len = P.seg_rowlen[(long long)s * MF_BS + i];
-        const unsigned long long *mrow = (const unsigned long long *)(P.meta + off + (long long)i * kp);
-        float part = 0.0f;
-        int prev = -1;
-        for (int k0 = 0; k0 < len; k0 += 8) {
-            const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
-            if (MODE == MODE_FP64 || force_pr == MF_P64) {
-                double vv[8], xx[8];
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const int k = k0 + j;
-                    const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
-                    const long long e = off + (long long)k * MF_BS + i;
-                    if (k < len) {
-                        vv[j] = __ldcs(P.v64 + e);
-                        xx[j] = x64[sh.xb[tb + (mm >> 4)] + (mm & 15u)];
-                    } else {
-                        vv[j] = 0.0;
-                        xx[j] = 0.0;
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < 8; j++) acc = fma(vv[j], xx[j], acc);
-            } else {
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const int k = k0 + j;
-                    if (k >= len) break;
-                    const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
-                    const int slot = (int)(mm >> 4);
-                    const long long e = off + (long long)k * MF_BS + i;
-                    const int xi = sh.xb[tb + slot] + (int)(mm & 15u);
-                    const int pr = sh.pr[tb + slot];
-                    if (slot != prev) {
-                        acc += (double)part;
-                        part = 0.0f;
-                        prev = slot;
-                    }
-                    if (pr == MF_P64) {
-                        acc = fma(__ldcs(P.v64 + e), x64[xi], acc);
-                    } else if (pr == MF_P32) {
-                        part = fmaf(__ldcs(P.v32 + e), x32[xi], part);
-                    } else if (pr == MF_P16) {
-                        part = fmaf(__half2float(P.v16[e]), x32[xi], part);
-                    } else if (pr == MF_P8) {
-                        part = fmaf((float)P.v8[e] * sh.sc[tb + slot], x32[xi], part);
-                    }
-                }
-            }
-        }
-        acc += (double)part;
-        __syncwarp(hmask);
     }
     return acc;
 }
 
+// Row i of one slice times x.  The 8 entries of a chunk are loaded together
+// (value + gathered x), then accumulated.  Occupancy (32 warps per SM) hides
+// the memory latency: measured on the 128^3 system this shape reaches ~73 % of
+// the HBM copy bandwidth, where a software-pipelined variant with twice the
+// registers per thread did not.  In mixed mode a slice runs in one precision,
+// the most conservative of its tiles' labels (no per-entry dispatch).
+template <int MODE, bool F64>
+__device__ __forceinline__ double slice_dot(const SolverParams &P, int4 h, int i, unsigned hmask, int len,
+                                            const TileReg &T, const XVec &X)
+{
+    const int kp = hdr_kp(h);
+    const long long off = hdr_off(h);
+    if (MODE == MODE_FP64 || F64) return slice_dot_uniform<MF_P64>(P, off, kp, i, hmask, len, T, X);
+    // precision codes order FP64 < FP32 < FP16 < INT8: the minimum is the most precise
+    int pr = (i < hdr_nt(h)) ? T.pr : MF_P8;
+#pragma unroll
+    for (int o = 8; o; o >>= 1) pr = min(pr, __shfl_xor_sync(hmask, pr, o));
+    if (pr == MF_P32) return slice_dot_uniform<MF_P32>(P, off, kp, i, hmask, len, T, X);
+    if (pr == MF_P64) return slice_dot_uniform<MF_P64>(P, off, kp, i, hmask, len, T, X);
+    if (pr == MF_P16) return slice_dot_uniform<MF_P16>(P, off, kp, i, hmask, len, T, X);
+    return slice_dot_uniform<MF_P8>(P, off, kp, i, hmask, len, T, X);
+}
+
+// Parity mode: the reference's tile arithmetic (main-cg-mixed.cu:1130-1214):
+// per (tile,row) two partial sums (even / odd entry positions, the lane pair of
+// the reference), each in the tile's precision -- FP64 fma, FP32 fmaf, FP16
+// __hfma on half x, INT8 in int8 on truncated x -- bypass tiles skipped; the
+// partials are added to the FP64 row sum, even then odd.
+__device__ __forceinline__ void parity_flush(double &acc, int pr, const double *a64, const float *a32,
+                                             const __half *a16, const int8_t *a8)
+{
+    for (int q = 0; q < 2; q++) {
+        if (pr == MF_P64) acc += a64[q];
+        else if (pr == MF_P32) acc += (double)a32[q];
+        else if (pr == MF_P16) acc += (double)__half2float(a16[q]);
+        else if (pr == MF_P8) acc += (double)a8[q];
+    }
+}
+
+__device__ __forceinline__ double slice_dot_parity(const SolverParams &P, int4 h, int i, unsigned hmask, int len,
+                                                   const TileReg &T, const XVec &X)
+{
+    const int kp = hdr_kp(h);
+    const long long off = hdr_off(h);
+    const unsigned char *mrow = P.meta + off + (long long)i * kp;
+    double acc = 0.0;
+    double a64[2] = {0.0, 0.0};
+    float a32[2] = {0.0f, 0.0f};
+    __half a16[2] = {__float2half_rn(0.0f), __float2half_rn(0.0f)};
+    int8_t a8[2] = {0, 0};
+    int cur_slot = -1, cur_pr = MF_PSKIP, pos = 0;
+    for (int k = 0; k < kp; k++) {
+        const bool act = k < len;
+        const unsigned mm = act ? (unsigned)mrow[k] : 0u;
+        const int slot = (int)(mm >> 4);
+        const int xi = __shfl_sync(hmask, T.xb, slot, 16) + (int)(mm & 15u);
+        const int pr = __shfl_sync(hmask, T.pr, slot, 16);
+        if (!act) continue;
+        if (slot != cur_slot) {
+            parity_flush(acc, cur_pr, a64, a32, a16, a8);
+            a64[0] = a64[1] = 0.0;
+            a32[0] = a32[1] = 0.0f;
+            a16[0] = a16[1] = __float2half_rn(0.0f);
+            a8[0] = a8[1] = 0;
+            cur_slot = slot;
+            cur_pr = pr;
+            pos = 0;
+        }
+        const long long e = off + (long long)k * MF_BS + i;
+        const int q = pos & 1;
+        if (pr == MF_P64) a64[q] = fma(X.x64[xi], P.v64[e], a64[q]);
+        else if (pr == MF_P32) a32[q] = fmaf(X.x32[xi], P.v32[e], a32[q]);
+        else if (pr == MF_P16) a16[q] = __hfma(X.x16[xi], P.v16[e], a16[q]);
+        else if (pr == MF_P8) a8[q] = (int8_t)((int)a8[q] + (int)X.x8[xi] * (int)P.v8ref[e]);
+        pos++;
+    }
+    parity_flush(acc, cur_pr, a64, a32, a16, a8);
+    return acc;
+}
+
+// y = A x over the half-warp's slices [sb, se); epi(R, y) is called once per
+// tile-row (after its last slice) with the row sum of lane i.
+// F64: every tile in FP64 (the FP64 residual replacement and the FP64 SpMV).
+template <int MODE, bool F64, typename Epi>
+__device__ __forceinline__ void spmv_range(const SolverParams &P, int sb, int se, int i, unsigned hmask,
+                                           const XVec &X, unsigned *cnt, Epi epi)
+{
+    double acc = 0.0;
+    for (int s = sb; s < se; s++) {
+        const int4 h = P.seg_hdr[s];
+        const TileReg T = load_tiles<MODE, F64>(P, h, i, X, cnt);
+        const int len = P.seg_rowlen[(long long)s * MF_BS + i];
+        if (MODE == MODE_PARITY && !F64) acc += slice_dot_parity(P, h, i, hmask, len, T, X);
+        else acc += slice_dot<MODE, F64>(P, h, i, hmask, len, T, X);
+        if (hdr_last(h)) {
+            epi(h.y, acc);
+            acc = 0.0;
+        }
+    }
+}
+
 // ------------------------------------------------------------ phases
 struct Ctx {
-    int lane, wib, half, i, tb, rbeg, rend;
+    int lane, wib, half, i, rbeg, rend, sbeg, send;
     unsigned hmask;
 };
 
@@ -278,15 +405,15 @@ __device__ __forceinline__ Ctx make_ctx(const SolverParams &P)
     c.wib = threadIdx.x >> 5;
     c.half = c.lane >> 4;
     c.i = c.lane & 15;
-    c.tb = c.wib * 32 + c.half * 16;
     c.hmask = 0xFFFFu << (16 * c.half);
     const int hw = (blockIdx.x * kWarps + c.wib) * 2 + c.half;
     c.rbeg = P.hw_begin[hw];
     c.rend = P.hw_begin[hw + 1];
+    c.sbeg = P.seg_ptr[c.rbeg];
+    c.send = P.seg_ptr[c.rend];
     return c;
 }
 
-// max over the 16 lanes of a half-warp
 // max over the 16 lanes of a half-warp; hmask names exactly those lanes (the
 // two halves of a warp walk different tile-row ranges, so they never shuffle together)
 __device__ __forceinline__ float half_max(float v, unsigned hmask)
@@ -317,11 +444,22 @@ __device__ __forceinline__ signed char rank_to_vis(int rank)
     return (signed char)(rank == 0 ? 1 : rank == 1 ? 2 : rank == 2 ? 3 : rank == 3 ? 4 : 0);
 }
 
-// Write a direction vector's FP32 shadow and segment statistics for the rows
-// of tile-row R (all 16 lanes of the half-warp call this together).
+// (int8_t) of a double as the x86-64 host compiler emits it (truncate to int32,
+// 0x80000000 when NaN / out of range, keep the low byte) -- the reference
+// converts p this way (main-cg-mixed.cu:464).
+__device__ __forceinline__ int8_t trunc_i8(double v)
+{
+    int w;
+    if (!(v == v) || v >= 2147483648.0 || v < -2147483648.0) w = (int)0x80000000u;
+    else w = (int)v;
+    return (int8_t)(unsigned char)(w & 0xFF);
+}
+
+// Write a direction vector's shadows and segment statistics for the rows of
+// tile-row R (all 16 lanes of the half-warp call this together).
 template <int MODE>
-__device__ __forceinline__ void publish_dir(const SolverParams &P, int R, int row, bool valid, double vnew,
-                                            double vold, float *v32, float *mag, signed char *lab, float &bmax,
+__device__ __forceinline__ void publish_dir(int R, int row, bool valid, double vnew, double vold, float *v32,
+                                            __half *v16, int8_t *v8, float *mag, signed char *lab, float &bmax,
                                             unsigned hmask, bool labels)
 {
     if (valid) v32[row] = (float)vnew;
@@ -329,25 +467,83 @@ __device__ __forceinline__ void publish_dir(const SolverParams &P, int R, int ro
         float m = half_max(valid ? (float)fabs(vnew) : 0.0f, hmask);
         bmax = fmaxf(bmax, m);
         if ((threadIdx.x & 15) == 0) mag[R] = m;
-    } else if (MODE == MODE_PARITY && labels) {
-        // reference rule: label of the next SpMV's tile column from |v_new - v_old|
-        int rk = half_max_i(valid ? ref_rank(fabs(vnew - vold)) : 0, hmask);
-        if ((threadIdx.x & 15) == 0) lab[R] = rank_to_vis(rk);
+    } else if (MODE == MODE_PARITY) {
+        if (valid) {
+            v16[row] = __double2half(vnew);
+            v8[row] = trunc_i8(vnew);
+        }
+        if (labels) {
+            // reference rule: label of the next SpMV's tile column from |v_new - v_old|
+            int rk = half_max_i(valid ? ref_rank(fabs(vnew - vold)) : 0, hmask);
+            if ((threadIdx.x & 15) == 0) lab[R] = rank_to_vis(rk);
+        }
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 2) k_solve(SolverParams P)
+__device__ __forceinline__ XVec make_x(const double *x64, const float *x32, const __half *x16, const int8_t *x8,
+                                       const float *mag, const signed char *lab, float invM)
+{
+    XVec X;
+    X.x64 = x64;
+    X.x32 = x32;
+    X.x16 = x16;
+    X.x8 = x8;
+    X.mag = mag;
+    X.lab = lab;
+    X.invM = invM;
+    X.force_pr = -1;
+    return X;
+}
+
+__device__ __forceinline__ XVec fp64_x(const double *x64)
+{
+    XVec X = make_x(x64, nullptr, nullptr, nullptr, nullptr, nullptr, 0.f);
+    X.force_pr = MF_P64;
+    return X;
+}
+
+// LB = minimum resident blocks per SM the register budget is sized for:
+// 1 -> up to 128 registers (no spills, 16 warps / SM), 2 -> 64 registers (32 warps / SM).
+// Block 0 / thread 0 splits its wall time into phases (%globaltimer deltas);
+// the state lives in shared memory so the other threads spend no registers on it.
+struct PhaseClock {
+    Shared *sh;
+    __device__ bool on() const { return blockIdx.x == 0 && threadIdx.x == 0; }
+    __device__ void start(Shared *s)
+    {
+        sh = s;
+        if (on()) {
+            sh->clk_t = mf_globaltimer();
+            for (int j = 0; j < 5; j++) sh->clk_acc[j] = 0ull;
+        }
+    }
+    __device__ void lap(int ph)
+    {
+        if (on()) {
+            const unsigned long long n = mf_globaltimer();
+            sh->clk_acc[ph] += n - sh->clk_t;
+            sh->clk_t = n;
+        }
+    }
+};
+enum { PH_SPMV = 0, PH_VECB = 1, PH_VECC = 2, PH_BAR = 3, PH_REPL = 4 };
+
+template <int MODE, int LB>
+__global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
 {
     __shared__ Shared sh;
     const Ctx c = make_ctx(P);
     unsigned epoch = 0;
-    unsigned long long cnt[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned *cnt = sh.cnt[c.wib];
+    if (c.lane < 10) cnt[c.lane] = 0u;
+    __syncwarp();
+    PhaseClock clk;
+    clk.start(&sh);
     const int n = P.n;
     const bool bicg = (P.method == MF_METHOD_BICGSTAB);
 
     // ---- init: x = 0 (owned rows), r = b, p = r (rh = r) ----
-    double pb = 0.0, pr1 = 0.0;
+    double pb = 0.0;
     float bmax = 0.0f;
     for (int R = c.rbeg; R < c.rend; R++) {
         const int row = R * MF_BS + c.i;
@@ -359,121 +555,81 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(SolverParams P)
             P.p[row] = bv;
             if (bicg) P.rh[row] = bv;
         }
-        publish_dir<MODE>(P, R, row, valid, bv, 0.0, P.p32, P.mag_p, P.lab_p, bmax, c.hmask, false);
+        // parity mode: labels start all FP64 (cudaMemset(d_vis, 0), main-cg-mixed.cu:2828)
+        publish_dir<MODE>(R, row, valid, bv, 0.0, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, false);
         pb += bv * bv;
     }
-    pr1 = pb;
-    block_partial(P, sh, 0, pb, pr1, (double)bmax, 0.0, 3, 0x4u);
+    block_partial(P, sh, 0, pb, (double)bmax, 0, 0, 2, 0x2u);
     if (!grid_barrier(P, epoch, sh)) return;
     double v[4];
-    grid_collect(P, sh, 0, 3, 0x4u, v);
+    grid_collect(P, sh, 0, 2, 0x2u, v);
+            clk.lap(PH_BAR);
     const double bb = v[0];
-    double rr = v[0], r1 = v[1];
-    float invM = v[2] > 0.0 ? (float)(1.0 / v[2]) : 0.0f;
+    double rr = v[0], r1 = v[0];
+    float invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
     float invMs = 0.0f;
-    // parity mode: initial labels are all FP64 (cudaMemset(d_vis, 0), main-cg-mixed.cu:2828)
     const double thr2 = P.tol * P.tol * bb;
     int k = 0, conv = 0, repl = 0, status = 0, last_true = 0;
     double rr_true = rr;
     if (!P.fixed_iters && rr <= thr2) { conv = 1; last_true = 1; }
 
-    // reference labels start at FP64 for p (d_vis zeroed)
     while (!conv && k < P.max_iter) {
+        double alpha = 0.0, omega = 0.0;
         if (!bicg) {
-            // ---- Phase A: q = A p, p.q ----
+            // ---- A: q = A p, p.q ----
             double ppq = 0.0;
-            for (int R = c.rbeg; R < c.rend; R++) {
-                const double y = spmv_row<MODE>(P, sh, R, c.i, c.tb, c.hmask, P.p, P.p32, P.mag_p, invM, P.lab_p,
-                                                -1, cnt);
-                const int row = R * MF_BS + c.i;
-                if (row < n) {
-                    P.q[row] = y;
-                    ppq += P.p[row] * y;
-                }
-            }
+            spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
+                             make_x(P.p, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, invM), cnt,
+                             [&](int R, double y) {
+                                 const int row = R * MF_BS + c.i;
+                                 if (row < n) {
+                                     P.q[row] = y;
+                                     ppq += P.p[row] * y;
+                                 }
+                             });
+            clk.lap(PH_SPMV);
             block_partial(P, sh, 1, ppq, 0, 0, 0, 1, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 1, 1, 0u, v);
-            const double alpha = rr / v[0];
+            clk.lap(PH_BAR);
+            alpha = rr / v[0];
             if (!isfinite(alpha)) { status = MF_ERR_BREAKDOWN; break; }
-            // ---- Phase B: x += alpha p, r -= alpha q, r.r ----
+            // ---- B: r -= alpha q, r.r  (x is updated with p in phase C) ----
             double prr = 0.0;
+#pragma unroll 4
             for (int R = c.rbeg; R < c.rend; R++) {
                 const int row = R * MF_BS + c.i;
                 if (row < n) {
-                    P.x[row] += alpha * P.p[row];
                     const double rv = P.r[row] - alpha * P.q[row];
                     P.r[row] = rv;
                     prr += rv * rv;
                 }
             }
+            clk.lap(PH_VECB);
             block_partial(P, sh, 2, prr, 0, 0, 0, 1, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 2, 1, 0u, v);
-            double rr_new = v[0];
-            k++;
-            last_true = 0;
-            const bool want_check = !P.fixed_iters && rr_new <= thr2;
-            const bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
-            if (want_check || want_repl) {
-                // ---- FP64 true residual: r = b - A x ----
-                double prt = 0.0;
-                for (int R = c.rbeg; R < c.rend; R++) {
-                    const double y = spmv_row<MODE>(P, sh, R, c.i, c.tb, c.hmask, P.x, nullptr, nullptr, 0.f,
-                                                    nullptr, MF_P64, nullptr);
-                    const int row = R * MF_BS + c.i;
-                    if (row < n) {
-                        const double rv = P.b[row] - y;
-                        P.r[row] = rv;
-                        prt += rv * rv;
-                    }
-                }
-                block_partial(P, sh, 3, prt, 0, 0, 0, 1, 0u);
-                if (!grid_barrier(P, epoch, sh)) return;
-                grid_collect(P, sh, 3, 1, 0u, v);
-                rr_new = v[0];
-                rr_true = rr_new;
-                repl++;
-                last_true = 1;
-                if (!P.fixed_iters && rr_new <= thr2) { rr = rr_new; conv = 1; break; }
-            }
-            const double beta = rr_new / rr;
-            rr = rr_new;
-            // ---- Phase C: p = r + beta p ----
-            bmax = 0.0f;
-            for (int R = c.rbeg; R < c.rend; R++) {
-                const int row = R * MF_BS + c.i;
-                const bool valid = row < n;
-                double pold = 0.0, pn = 0.0;
-                if (valid) {
-                    pold = P.p[row];
-                    pn = P.r[row] + beta * pold;
-                    P.p[row] = pn;
-                }
-                publish_dir<MODE>(P, R, row, valid, pn, pold, P.p32, P.mag_p, P.lab_p, bmax, c.hmask, true);
-            }
-            block_partial(P, sh, 4, (double)bmax, 0, 0, 0, 1, 0x1u);
-            if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 4, 1, 0x1u, v);
-            invM = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
+            clk.lap(PH_BAR);
         } else {
-            // ---- BiCGSTAB: v = A p, alpha = r1 / (rh.v) ----
+            // ---- BiCGSTAB A1: v = A p, alpha = r1 / (rh.v) ----
             double prv = 0.0;
-            for (int R = c.rbeg; R < c.rend; R++) {
-                const double y = spmv_row<MODE>(P, sh, R, c.i, c.tb, c.hmask, P.p, P.p32, P.mag_p, invM, P.lab_p,
-                                                -1, cnt);
-                const int row = R * MF_BS + c.i;
-                if (row < n) {
-                    P.q[row] = y;
-                    prv += P.rh[row] * y;
-                }
-            }
+            spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
+                             make_x(P.p, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, invM), cnt,
+                             [&](int R, double y) {
+                                 const int row = R * MF_BS + c.i;
+                                 if (row < n) {
+                                     P.q[row] = y;
+                                     prv += P.rh[row] * y;
+                                 }
+                             });
+            clk.lap(PH_SPMV);
             block_partial(P, sh, 1, prv, 0, 0, 0, 1, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 1, 1, 0u, v);
-            const double alpha = r1 / v[0];
+            clk.lap(PH_BAR);
+            alpha = r1 / v[0];
             if (!isfinite(alpha)) { status = MF_ERR_BREAKDOWN; break; }
-            // s = r - alpha v
+            // ---- B1: s = r - alpha v ----
             float smax = 0.0f;
             for (int R = c.rbeg; R < c.rend; R++) {
                 const int row = R * MF_BS + c.i;
@@ -484,30 +640,36 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(SolverParams P)
                     sn = P.r[row] - alpha * P.q[row];
                     P.s[row] = sn;
                 }
-                publish_dir<MODE>(P, R, row, valid, sn, sold, P.s32, P.mag_s, P.lab_s, smax, c.hmask, true);
+                publish_dir<MODE>(R, row, valid, sn, sold, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, smax, c.hmask,
+                                  true);
             }
+            clk.lap(PH_VECB);
             block_partial(P, sh, 2, (double)smax, 0, 0, 0, 1, 0x1u);
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 2, 1, 0x1u, v);
+            clk.lap(PH_BAR);
             invMs = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
-            // t = A s, omega = (t.s)/(t.t)
+            // ---- A2: t = A s, omega = (t.s)/(t.t) ----
             double pts = 0.0, ptt = 0.0;
-            for (int R = c.rbeg; R < c.rend; R++) {
-                const double y = spmv_row<MODE>(P, sh, R, c.i, c.tb, c.hmask, P.s, P.s32, P.mag_s, invMs, P.lab_s,
-                                                -1, cnt);
-                const int row = R * MF_BS + c.i;
-                if (row < n) {
-                    P.t[row] = y;
-                    pts += y * P.s[row];
-                    ptt += y * y;
-                }
-            }
+            spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
+                             make_x(P.s, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, invMs), cnt,
+                             [&](int R, double y) {
+                                 const int row = R * MF_BS + c.i;
+                                 if (row < n) {
+                                     P.t[row] = y;
+                                     pts += y * P.s[row];
+                                     ptt += y * y;
+                                 }
+                             });
+            clk.lap(PH_SPMV);
             block_partial(P, sh, 3, pts, ptt, 0, 0, 2, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 3, 2, 0u, v);
-            const double omega = (v[1] != 0.0) ? v[0] / v[1] : 0.0;
-            // x += alpha p + omega s; r = s - omega t
+            clk.lap(PH_BAR);
+            omega = (v[1] != 0.0) ? v[0] / v[1] : 0.0;
+            // ---- B2: x += alpha p + omega s; r = s - omega t ----
             double prr = 0.0, prh = 0.0;
+#pragma unroll 2
             for (int R = c.rbeg; R < c.rend; R++) {
                 const int row = R * MF_BS + c.i;
                 if (row < n) {
@@ -519,83 +681,118 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(SolverParams P)
                     prh += rv * P.rh[row];
                 }
             }
+            clk.lap(PH_VECB);
             block_partial(P, sh, 4, prr, prh, 0, 0, 2, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 4, 2, 0u, v);
-            double rr_new = v[0], r1_new = v[1];
-            k++;
-            last_true = 0;
-            const bool want_check = !P.fixed_iters && rr_new <= thr2;
-            const bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
-            if (want_check || want_repl) {
-                double prt = 0.0, prth = 0.0;
-                for (int R = c.rbeg; R < c.rend; R++) {
-                    const double y = spmv_row<MODE>(P, sh, R, c.i, c.tb, c.hmask, P.x, nullptr, nullptr, 0.f,
-                                                    nullptr, MF_P64, nullptr);
-                    const int row = R * MF_BS + c.i;
-                    if (row < n) {
-                        const double rv = P.b[row] - y;
-                        P.r[row] = rv;
-                        prt += rv * rv;
-                        prth += rv * P.rh[row];
-                    }
-                }
-                block_partial(P, sh, 5, prt, prth, 0, 0, 2, 0u);
-                if (!grid_barrier(P, epoch, sh)) return;
-                grid_collect(P, sh, 5, 2, 0u, v);
-                rr_new = v[0];
-                r1_new = v[1];
-                rr_true = rr_new;
-                repl++;
-                last_true = 1;
-                if (!P.fixed_iters && rr_new <= thr2) { rr = rr_new; conv = 1; break; }
-            }
-            const double beta = (r1_new * alpha) / (r1 * omega);
-            rr = rr_new;
-            r1 = r1_new;
-            if (!isfinite(beta)) { status = MF_ERR_BREAKDOWN; break; }
-            // p = r + beta (p - omega v)
-            bmax = 0.0f;
-            for (int R = c.rbeg; R < c.rend; R++) {
-                const int row = R * MF_BS + c.i;
-                const bool valid = row < n;
-                double pold = 0.0, pn = 0.0;
-                if (valid) {
-                    pold = P.p[row];
-                    pn = P.r[row] + beta * (pold - omega * P.q[row]);
-                    P.p[row] = pn;
-                }
-                publish_dir<MODE>(P, R, row, valid, pn, pold, P.p32, P.mag_p, P.lab_p, bmax, c.hmask, true);
-            }
-            block_partial(P, sh, 6, (double)bmax, 0, 0, 0, 1, 0x1u);
-            if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 6, 1, 0x1u, v);
-            invM = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
+            clk.lap(PH_BAR);
         }
+        double rr_new = v[0], r1_new = bicg ? v[1] : 0.0;
+        k++;
+        last_true = 0;
+        bool x_done = bicg;      // CG defers x += alpha p to phase C
+        const bool want_check = !P.fixed_iters && rr_new <= thr2;
+        const bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
+        if (want_check || want_repl) {
+            if (!x_done) {
+                // the FP64 residual needs the current x: apply this iteration's step first
+                for (int R = c.rbeg; R < c.rend; R++) {
+                    const int row = R * MF_BS + c.i;
+                    if (row < n) P.x[row] += alpha * P.p[row];
+                }
+                x_done = true;
+                if (!grid_barrier(P, epoch, sh)) return;
+            }
+            // ---- FP64 true residual: r = b - A x ----
+            double prt = 0.0, prth = 0.0;
+            spmv_range<MODE, true>(P, c.sbeg, c.send, c.i, c.hmask, fp64_x(P.x), nullptr, [&](int R, double y) {
+                const int row = R * MF_BS + c.i;
+                if (row < n) {
+                    const double rv = P.b[row] - y;
+                    P.r[row] = rv;
+                    prt += rv * rv;
+                    if (bicg) prth += rv * P.rh[row];
+                }
+            });
+            // rows of tile-rows without tiles (A row = 0): r = b there
+            for (int R = c.rbeg; R < c.rend; R++) {
+                if (P.seg_ptr[R] != P.seg_ptr[R + 1]) continue;
+                const int row = R * MF_BS + c.i;
+                if (row < n) {
+                    const double rv = P.b[row];
+                    P.r[row] = rv;
+                    prt += rv * rv;
+                    if (bicg) prth += rv * P.rh[row];
+                }
+            }
+            clk.lap(PH_REPL);
+            block_partial(P, sh, 5, prt, prth, 0, 0, 2, 0u);
+            if (!grid_barrier(P, epoch, sh)) return;
+            grid_collect(P, sh, 5, 2, 0u, v);
+            clk.lap(PH_BAR);
+            rr_new = v[0];
+            r1_new = v[1];
+            rr_true = rr_new;
+            repl++;
+            last_true = 1;
+            if (!P.fixed_iters && rr_new <= thr2) { rr = rr_new; conv = 1; break; }
+        }
+        // ---- C: (CG: x += alpha p,) p = r + beta p  /  p = r + beta (p - omega v) ----
+        double beta;
+        if (!bicg) {
+            beta = rr_new / rr;
+        } else {
+            beta = (r1_new * alpha) / (r1 * omega);
+            r1 = r1_new;
+            if (!isfinite(beta)) { rr = rr_new; status = MF_ERR_BREAKDOWN; break; }
+        }
+        rr = rr_new;
+        bmax = 0.0f;
+        for (int R = c.rbeg; R < c.rend; R++) {
+            const int row = R * MF_BS + c.i;
+            const bool valid = row < n;
+            double pold = 0.0, pn = 0.0;
+            if (valid) {
+                pold = P.p[row];
+                if (!x_done) P.x[row] += alpha * pold;
+                pn = bicg ? P.r[row] + beta * (pold - omega * P.q[row]) : P.r[row] + beta * pold;
+                P.p[row] = pn;
+            }
+            publish_dir<MODE>(R, row, valid, pn, pold, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, true);
+        }
+        clk.lap(PH_VECC);
+        block_partial(P, sh, 6, (double)bmax, 0, 0, 0, 1, 0x1u);
+        if (!grid_barrier(P, epoch, sh)) return;
+        grid_collect(P, sh, 6, 1, 0x1u, v);
+            clk.lap(PH_BAR);
+        invM = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
     }
     // ---- final FP64 true residual when the last one was not already formed ----
     if (!last_true) {
         double prt = 0.0;
-        for (int R = c.rbeg; R < c.rend; R++) {
-            const double y = spmv_row<MODE>(P, sh, R, c.i, c.tb, c.hmask, P.x, nullptr, nullptr, 0.f, nullptr,
-                                            MF_P64, nullptr);
+        spmv_range<MODE, true>(P, c.sbeg, c.send, c.i, c.hmask, fp64_x(P.x), nullptr, [&](int R, double y) {
             const int row = R * MF_BS + c.i;
             if (row < n) {
                 const double d = P.b[row] - y;
                 prt += d * d;
             }
+        });
+        for (int R = c.rbeg; R < c.rend; R++) {
+            if (P.seg_ptr[R] != P.seg_ptr[R + 1]) continue;
+            const int row = R * MF_BS + c.i;
+            if (row < n) prt += P.b[row] * P.b[row];
         }
         block_partial(P, sh, 7, prt, 0, 0, 0, 1, 0u);
         if (!grid_barrier(P, epoch, sh)) return;
         grid_collect(P, sh, 7, 1, 0u, v);
+            clk.lap(PH_BAR);
         rr_true = v[0];
     }
     // tile-use counters
-    for (int j = 0; j < 10; j++) {
-        unsigned long long a = cnt[j];
-        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-        if (c.lane == 0 && a) atomicAdd(&P.counts[j], a);
-    }
+    __syncwarp();
+    if (c.lane < 10 && cnt[c.lane]) atomicAdd(&P.counts[c.lane], (unsigned long long)cnt[c.lane]);
+    if (clk.on() && P.phase_ns)
+        for (int j = 0; j < 5; j++) P.phase_ns[j] = sh.clk_acc[j];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         P.out[0] = (double)k;
         P.out[1] = (double)conv;
@@ -608,20 +805,27 @@ __global__ void __launch_bounds__(kThreads, 2) k_solve(SolverParams P)
 }
 
 // ------------------------------------------------------------ standalone SpMV
-template <int MODE>
-__global__ void __launch_bounds__(kThreads) k_spmv(SolverParams P, int force_pr, double *y)
+// y = A x, one half-warp per tile-row range (same pipeline as the solver).
+template <int MODE, int LB>
+__global__ void __launch_bounds__(kThreads, LB) k_spmv(SolverParams P, int force_pr, double *y, int rows_per_hw)
 {
-    __shared__ Shared sh;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, half = lane >> 4, i = lane & 15;
-    const int tb = wib * 32 + half * 16;
     const unsigned hmask = 0xFFFFu << (16 * half);
     const int hw = (blockIdx.x * kWarps + wib) * 2 + half;
-    const int nhw = gridDim.x * kWarps * 2;
-    for (int R = hw; R < P.tilem; R += nhw) {
-        const double v = spmv_row<MODE>(P, sh, R, i, tb, hmask, P.x, P.p32, nullptr, 0.f, nullptr, force_pr,
-                                        nullptr);
+    const int rb = min(P.tilem, hw * rows_per_hw), re = min(P.tilem, rb + rows_per_hw);
+    if (rb >= re) return;
+    XVec X = make_x(P.x, P.p32, nullptr, nullptr, nullptr, nullptr, 0.f);
+    X.force_pr = force_pr;
+    const int n = P.n;
+    spmv_range<MODE, MODE == MODE_FP64>(P, P.seg_ptr[rb], P.seg_ptr[re], i, hmask, X, nullptr,
+                                        [&](int R, double v) {
         const int row = R * MF_BS + i;
-        if (row < P.n) y[row] = v;
+        if (row < n) y[row] = v;
+    });
+    for (int R = rb; R < re; R++) {          // tile-rows without tiles: y = 0
+        if (P.seg_ptr[R] != P.seg_ptr[R + 1]) continue;
+        const int row = R * MF_BS + i;
+        if (row < n) y[row] = 0.0;
     }
 }
 
@@ -661,15 +865,22 @@ __global__ void k_ref_labels(const double *pold, const double *pnew, int nseg, i
 // ------------------------------------------------------------ workspace
 struct Workspace {
     int G;                 // grid blocks of the persistent kernel
-    int mode;
+    int lb;                // register-budget variant (blocks per SM it was built for)
+    // every solver vector lives in one block, hot CG set first, so one L2
+    // access-policy window covers it:  p32 | p | q | r | x | s32 | s | t | rh | p16 s16 p8 s8
+    char *vecs;
+    size_t cg_bytes, all_bytes;
     double *r, *p, *q, *rh, *s, *t, *x;
     float *p32, *s32, *mag_p, *mag_s;
+    __half *p16, *s16;
+    int8_t *p8, *s8;
     signed char *lab_p, *lab_s;
     double *red;
     unsigned int *bar;
     int *err;
     double *out;
     unsigned long long *counts;
+    unsigned long long *phase_ns;
     int *hw_begin;
     int nhw;
     cudaEvent_t e0, e1;
@@ -688,15 +899,22 @@ int dal(T **p, long long count)
         if (_rc != MF_SUCCESS) return _rc;  \
     } while (0)
 
-const void *solve_kernel(int mode)
+const void *solve_kernel(int mode, int lb)
 {
-    if (mode == MODE_FP64) return (const void *)k_solve<MODE_FP64>;
-    if (mode == MODE_MIXED) return (const void *)k_solve<MODE_MIXED>;
-    return (const void *)k_solve<MODE_PARITY>;
+    if (lb == 2) {
+        if (mode == MODE_FP64) return (const void *)k_solve<MODE_FP64, 2>;
+        if (mode == MODE_MIXED) return (const void *)k_solve<MODE_MIXED, 2>;
+        return (const void *)k_solve<MODE_PARITY, 2>;
+    }
+    if (mode == MODE_FP64) return (const void *)k_solve<MODE_FP64, 1>;
+    if (mode == MODE_MIXED) return (const void *)k_solve<MODE_MIXED, 1>;
+    return (const void *)k_solve<MODE_PARITY, 1>;
 }
 
-int ws_get(mf_matrix_s *A, int mode, int blocks_per_sm, Workspace **out, cudaStream_t s)
+int ws_get(mf_matrix_s *A, int blocks_per_sm, Workspace **out, cudaStream_t s)
 {
+    // blocks_per_sm: 0 = default variant, 1 or 2 = that register-budget variant
+    const int lb = (blocks_per_sm == 2) ? 2 : (blocks_per_sm == 1) ? 1 : kDefaultLB;
     int dev = 0;
     MF_CUDA_TRY(cudaGetDevice(&dev));
     int nsm = 0;
@@ -708,18 +926,17 @@ int ws_get(mf_matrix_s *A, int mode, int blocks_per_sm, Workspace **out, cudaStr
     int occ = 1 << 20;
     for (int m = MODE_FP64; m <= MODE_PARITY; m++) {
         int o = 0;
-        MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, solve_kernel(m), kThreads, 0));
+        MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, solve_kernel(m, lb), kThreads, 0));
         occ = o < occ ? o : occ;
     }
-    (void)mode;
     if (occ < 1) return MF_ERR_UNSUPPORTED;
-    if (blocks_per_sm > 0 && blocks_per_sm < occ) occ = blocks_per_sm;
+    if (occ > lb) occ = lb;
     int G = nsm * occ;
     // small systems: no more blocks than needed for one tile-row per half-warp
     const int need = (A->tilem + kWarps * 2 - 1) / (kWarps * 2);
     if (need < G) G = need > 0 ? need : 1;
     Workspace *w = (Workspace *)A->ws;
-    if (w && w->G == G) {
+    if (w && w->G == G && w->lb == lb) {
         *out = w;
         return MF_SUCCESS;
     }
@@ -727,16 +944,35 @@ int ws_get(mf_matrix_s *A, int mode, int blocks_per_sm, Workspace **out, cudaStr
     w = new Workspace();
     memset(w, 0, sizeof(*w));
     w->G = G;
+    w->lb = lb;
     const long long L = A->vec_len;
     const long long S = std::max(A->tilem, A->tilen) + 1;
-    MF_TRY(dal(&w->r, L)); MF_TRY(dal(&w->p, L)); MF_TRY(dal(&w->q, L)); MF_TRY(dal(&w->rh, L));
-    MF_TRY(dal(&w->s, L)); MF_TRY(dal(&w->t, L)); MF_TRY(dal(&w->x, L));
-    MF_TRY(dal(&w->p32, L)); MF_TRY(dal(&w->s32, L));
+    {
+        const size_t f = (size_t)L * sizeof(float), d = (size_t)L * sizeof(double), h = (size_t)L * sizeof(__half);
+        w->cg_bytes = f + 4 * d;
+        w->all_bytes = w->cg_bytes + f + 3 * d + 2 * h + 2 * (size_t)L;
+        MF_CUDA_TRY(cudaMalloc((void **)&w->vecs, w->all_bytes));
+        char *c = w->vecs;
+        w->p32 = (float *)c; c += f;
+        w->p = (double *)c; c += d;
+        w->q = (double *)c; c += d;
+        w->r = (double *)c; c += d;
+        w->x = (double *)c; c += d;
+        w->s32 = (float *)c; c += f;
+        w->s = (double *)c; c += d;
+        w->t = (double *)c; c += d;
+        w->rh = (double *)c; c += d;
+        w->p16 = (__half *)c; c += h;
+        w->s16 = (__half *)c; c += h;
+        w->p8 = (int8_t *)c; c += L;
+        w->s8 = (int8_t *)c;
+    }
     MF_TRY(dal(&w->mag_p, S)); MF_TRY(dal(&w->mag_s, S));
     MF_TRY(dal(&w->lab_p, S)); MF_TRY(dal(&w->lab_s, S));
     MF_TRY(dal(&w->red, (long long)kRedKinds * G * kRedWidth));
     MF_TRY(dal(&w->bar, 1)); MF_TRY(dal(&w->err, 1)); MF_TRY(dal(&w->out, 16));
     MF_TRY(dal(&w->counts, 16));
+    MF_TRY(dal(&w->phase_ns, 8));
     w->nhw = G * kWarps * 2;
     MF_TRY(dal(&w->hw_begin, w->nhw + 1));
     MF_CUDA_TRY(cudaEventCreate(&w->e0));
@@ -755,15 +991,14 @@ void fill_params(SolverParams &P, mf_matrix_s *A, Workspace *w)
     P.tilem = A->tilem;
     P.vec_len = A->vec_len;
     P.seg_ptr = A->d_seg_ptr;
-    P.seg_tile0 = A->d_seg_tile0;
-    P.seg_kp = A->d_seg_kp;
-    P.seg_off = A->d_seg_off;
+    P.seg_hdr = A->d_seg_hdr;
     P.seg_rowlen = A->d_seg_rowlen;
     P.meta = A->d_meta;
     P.v64 = A->d_v64;
     P.v32 = A->d_v32;
     P.v16 = A->d_v16;
     P.v8 = A->d_v8;
+    P.v8ref = A->d_v8ref;
     P.tile_col = A->d_tile_columnidx;
     P.tile_off = A->d_csr_offset;
     P.i8_scale = A->d_i8_scale;
@@ -771,11 +1006,63 @@ void fill_params(SolverParams &P, mf_matrix_s *A, Workspace *w)
     if (w) {
         P.hw_begin = w->hw_begin;
         P.x = w->x; P.r = w->r; P.p = w->p; P.q = w->q; P.rh = w->rh; P.s = w->s; P.t = w->t;
-        P.p32 = w->p32; P.s32 = w->s32; P.mag_p = w->mag_p; P.mag_s = w->mag_s;
-        P.lab_p = w->lab_p; P.lab_s = w->lab_s;
+        P.p32 = w->p32; P.s32 = w->s32; P.p16 = w->p16; P.s16 = w->s16; P.p8 = w->p8; P.s8 = w->s8;
+        P.mag_p = w->mag_p; P.mag_s = w->mag_s; P.lab_p = w->lab_p; P.lab_s = w->lab_s;
         P.red = w->red; P.bar = w->bar; P.err = w->err; P.out = w->out; P.counts = w->counts;
+        P.phase_ns = w->phase_ns;
     }
 }
+
+// Persisting L2 access-policy window on a stream for the duration of a solve.
+struct L2Window {
+    bool active = false;
+    size_t old_limit = 0;
+    cudaStreamAttrValue old_attr;
+    void set(cudaStream_t s, void *base, size_t bytes)
+    {
+        int dev = 0, max_persist = 0, max_win = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return;
+        if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
+            max_persist <= 0 || max_win <= 0) {
+            cudaGetLastError();
+            return;
+        }
+        if (cudaStreamGetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &old_attr) != cudaSuccess ||
+            cudaDeviceGetLimit(&old_limit, cudaLimitPersistingL2CacheSize) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        const size_t win = bytes < (size_t)max_win ? bytes : (size_t)max_win;
+        const size_t lim = win < (size_t)max_persist ? win : (size_t)max_persist;
+        if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        cudaStreamAttrValue a;
+        memset(&a, 0, sizeof(a));
+        a.accessPolicyWindow.base_ptr = base;
+        a.accessPolicyWindow.num_bytes = win;
+        a.accessPolicyWindow.hitRatio = (float)((double)lim / (double)win);
+        a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        if (cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &a) != cudaSuccess) {
+            cudaGetLastError();
+            cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, old_limit);
+            return;
+        }
+        active = true;
+    }
+    void reset(cudaStream_t s)
+    {
+        if (!active) return;
+        cudaStreamSetAttribute(s, cudaStreamAttributeAccessPolicyWindow, &old_attr);
+        cudaCtxResetPersistingL2Cache();
+        cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, old_limit);
+        cudaGetLastError();
+        active = false;
+    }
+};
 
 }  // namespace
 
@@ -783,11 +1070,12 @@ void mf_solver_free_ws(mf_matrix_s *A)
 {
     Workspace *w = (Workspace *)A->ws;
     if (!w) return;
-    cudaFree(w->r); cudaFree(w->p); cudaFree(w->q); cudaFree(w->rh); cudaFree(w->s); cudaFree(w->t);
-    cudaFree(w->x); cudaFree(w->p32); cudaFree(w->s32); cudaFree(w->mag_p); cudaFree(w->mag_s);
-    cudaFree(w->lab_p); cudaFree(w->lab_s); cudaFree(w->red); cudaFree(w->bar); cudaFree(w->err);
-    cudaFree(w->out); cudaFree(w->counts); cudaFree(w->hw_begin);
-    cudaEventDestroy(w->e0); cudaEventDestroy(w->e1);
+    void *ptrs[] = {w->vecs, w->mag_p, w->mag_s, w->lab_p, w->lab_s, w->red, w->bar, w->err, w->out, w->counts,
+                    w->phase_ns, w->hw_begin};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    cudaEventDestroy(w->e0);
+    cudaEventDestroy(w->e1);
     delete w;
     A->ws = nullptr;
 }
@@ -800,15 +1088,23 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     if (opt->method != MF_METHOD_CG && opt->method != MF_METHOD_BICGSTAB) return MF_ERR_INVALID;
     if (opt->x0_given) return MF_ERR_UNSUPPORTED;
     Workspace *w = nullptr;
-    MF_TRY(ws_get(A, mode, opt->blocks_per_sm, &w, s));
+    MF_TRY(ws_get(A, opt->blocks_per_sm, &w, s));
     const long long L = A->vec_len;
     const long long S = std::max(A->tilem, A->tilen) + 1;
     // zero the padded tails and the state the kernel reads before writing
     MF_CUDA_TRY(cudaMemsetAsync(w->x, 0, L * sizeof(double), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->p, 0, L * sizeof(double), s));
+    MF_CUDA_TRY(cudaMemsetAsync(w->q, 0, L * sizeof(double), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->s, 0, L * sizeof(double), s));
+    MF_CUDA_TRY(cudaMemsetAsync(w->t, 0, L * sizeof(double), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->p32, 0, L * sizeof(float), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->s32, 0, L * sizeof(float), s));
+    if (mode == MODE_PARITY) {
+        MF_CUDA_TRY(cudaMemsetAsync(w->p16, 0, L * sizeof(__half), s));
+        MF_CUDA_TRY(cudaMemsetAsync(w->s16, 0, L * sizeof(__half), s));
+        MF_CUDA_TRY(cudaMemsetAsync(w->p8, 0, L, s));
+        MF_CUDA_TRY(cudaMemsetAsync(w->s8, 0, L, s));
+    }
     MF_CUDA_TRY(cudaMemsetAsync(w->mag_p, 0, S * sizeof(float), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->mag_s, 0, S * sizeof(float), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->lab_p, 0, S, s));
@@ -817,6 +1113,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     MF_CUDA_TRY(cudaMemsetAsync(w->err, 0, sizeof(int), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->out, 0, 16 * sizeof(double), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->counts, 0, 16 * sizeof(unsigned long long), s));
+    MF_CUDA_TRY(cudaMemsetAsync(w->phase_ns, 0, 8 * sizeof(unsigned long long), s));
     SolverParams P;
     fill_params(P, A, w);
     P.b = d_b;
@@ -832,8 +1129,17 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     P.timeout_ns = (unsigned long long)(to * 1e9);
     P.stall_first_barrier = opt->test_stall_barrier ? 1 : 0;
     void *args[] = {&P};
+    // Keep the iteration vectors in L2 while the matrix payload streams past
+    // them: a persisting access-policy window over the vector block (best
+    // effort; the previous stream attribute and context limit are restored).
+    L2Window win;
+    if (opt->l2_window) win.set(s, w->vecs, opt->method == MF_METHOD_BICGSTAB ? w->all_bytes : w->cg_bytes);
     MF_CUDA_TRY(cudaEventRecord(w->e0, s));
-    MF_CUDA_TRY(cudaLaunchCooperativeKernel(solve_kernel(mode), dim3(w->G), dim3(kThreads), args, 0, s));
+    cudaError_t lerr = cudaLaunchCooperativeKernel(solve_kernel(mode, w->lb), dim3(w->G), dim3(kThreads), args, 0, s);
+    if (lerr != cudaSuccess) {
+        win.reset(s);
+        MF_CUDA_TRY(lerr);
+    }
     MF_CUDA_TRY(cudaEventRecord(w->e1, s));
     double out[16];
     unsigned long long counts[16];
@@ -841,8 +1147,11 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     MF_CUDA_TRY(cudaMemcpyAsync(out, w->out, sizeof(out), cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaMemcpyAsync(counts, w->counts, sizeof(counts), cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaMemcpyAsync(&err, w->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    unsigned long long phase[8];
+    MF_CUDA_TRY(cudaMemcpyAsync(phase, w->phase_ns, sizeof(phase), cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaMemcpyAsync(d_x, w->x, (size_t)A->n_rows * sizeof(double), cudaMemcpyDeviceToDevice, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
+    win.reset(s);
     float ms = 0.f;
     MF_CUDA_TRY(cudaEventElapsedTime(&ms, w->e0, w->e1));
     if (rep) {
@@ -860,6 +1169,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
         for (int j = 0; j < 4; j++) rep->tile_uses[j] = (long long)counts[j];
         rep->tiles_skipped = (long long)counts[4];
         for (int j = 0; j < 4; j++) rep->nnz_uses[j] = (long long)counts[5 + j];
+        for (int j = 0; j < 6; j++) rep->phase_ms[j] = (double)phase[j] * 1e-6;
     }
     if (err) return err;
     return (int)out[6];
@@ -869,7 +1179,7 @@ int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, c
 {
     // x is read through a padded copy so that column tiles past n_rows read zeros
     Workspace *w = nullptr;
-    MF_TRY(ws_get(A, MODE_FP64, 0, &w, s));
+    MF_TRY(ws_get(A, 0, &w, s));
     const long long L = A->vec_len;
     MF_CUDA_TRY(cudaMemsetAsync(w->x, 0, L * sizeof(double), s));
     MF_CUDA_TRY(cudaMemcpyAsync(w->x, d_x, (size_t)A->n_cols * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -880,15 +1190,21 @@ int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, c
     int nsm = 0, dev = 0;
     MF_CUDA_TRY(cudaGetDevice(&dev));
     MF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const int hw_per_block = kWarps * 2;
-    int blocks = (A->tilem + hw_per_block - 1) / hw_per_block;
-    const int cap = nsm * 4;
-    if (blocks > cap) blocks = cap;
-    if (blocks < 1) blocks = 1;
+    // one wave: resident blocks x SMs, each half-warp a contiguous range of tile-rows
     const int fpr = precision == MF_PREC_FP64 ? MF_P64 : MF_P32;
+    const void *kfn = fpr == MF_P64 ? (const void *)k_spmv<MODE_FP64, 2> : (const void *)k_spmv<MODE_MIXED, 2>;
+    int occ = 1;
+    MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kThreads, 0));
+    if (occ < 1) occ = 1;
+    const int nhw_max = nsm * occ * kWarps * 2;
+    int rows_per_hw = (A->tilem + nhw_max - 1) / nhw_max;
+    if (rows_per_hw < 1) rows_per_hw = 1;
+    const int nhw = (A->tilem + rows_per_hw - 1) / rows_per_hw;
+    int blocks = (nhw + kWarps * 2 - 1) / (kWarps * 2);
+    if (blocks < 1) blocks = 1;
     MF_CUDA_TRY(cudaEventRecord(w->e0, s));
-    if (fpr == MF_P64) k_spmv<MODE_FP64><<<blocks, kThreads, 0, s>>>(P, MF_P64, d_y);
-    else k_spmv<MODE_MIXED><<<blocks, kThreads, 0, s>>>(P, MF_P32, d_y);
+    if (fpr == MF_P64) k_spmv<MODE_FP64, 2><<<blocks, kThreads, 0, s>>>(P, MF_P64, d_y, rows_per_hw);
+    else k_spmv<MODE_MIXED, 2><<<blocks, kThreads, 0, s>>>(P, MF_P32, d_y, rows_per_hw);
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaEventRecord(w->e1, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));

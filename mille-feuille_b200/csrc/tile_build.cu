@@ -466,9 +466,9 @@ __global__ void k_seg_fill(const int *__restrict__ tile_ptr, const int *__restri
                            const int *__restrict__ csr_offset, const int *__restrict__ csrptr_offset,
                            const unsigned char *__restrict__ tptr, const unsigned char *__restrict__ tcol,
                            const double *__restrict__ tval, const float *__restrict__ tval_low,
-                           const int8_t *__restrict__ q8, int tilem, int rowA, unsigned char *__restrict__ meta,
-                           double *__restrict__ v64, float *__restrict__ v32, __half *__restrict__ v16,
-                           int8_t *__restrict__ v8)
+                           const int8_t *__restrict__ q8, const int8_t *__restrict__ q8ref, int tilem, int rowA,
+                           unsigned char *__restrict__ meta, double *__restrict__ v64, float *__restrict__ v32,
+                           __half *__restrict__ v16, int8_t *__restrict__ v8, int8_t *__restrict__ v8ref)
 {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -498,6 +498,7 @@ __global__ void k_seg_fill(const int *__restrict__ tile_ptr, const int *__restri
                         v32[pe] = tval_low[e];
                         v16[pe] = __float2half_rn(tval_low[e]);
                         v8[pe] = q8[e];
+                        v8ref[pe] = q8ref[e];
                         k++;
                     }
                 }
@@ -505,9 +506,25 @@ __global__ void k_seg_fill(const int *__restrict__ tile_ptr, const int *__restri
             for (; k < kp; k++) {
                 meta[off + (long long)i * kp + k] = 0;
                 long long pe = off + (long long)k * MF_BS + i;
-                v64[pe] = 0.0; v32[pe] = 0.0f; v16[pe] = __float2half_rn(0.0f); v8[pe] = 0;
+                v64[pe] = 0.0; v32[pe] = 0.0f; v16[pe] = __float2half_rn(0.0f); v8[pe] = 0; v8ref[pe] = 0;
             }
         }
+    }
+}
+
+// Packed per-segment header read once per segment by the solver's pipeline:
+// {first tile, tile-row, Kp | ntiles << 16 | last-slice-of-tile-row << 24,
+// entry offset / 128} (offsets are multiples of 128: Kp is a multiple of 8, 16 rows).
+__global__ void k_seg_hdr(const int *__restrict__ seg_ptr, const int *__restrict__ seg_tile0,
+                          const int *__restrict__ seg_kp, const long long *__restrict__ seg_off, int tilem,
+                          int4 *__restrict__ hdr)
+{
+    int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= tilem) return;
+    for (int s = seg_ptr[R]; s < seg_ptr[R + 1]; s++) {
+        const int nt = seg_tile0[s + 1] - seg_tile0[s];
+        const int last = (s + 1 == seg_ptr[R + 1]) ? 1 : 0;     // last slice of its tile-row
+        hdr[s] = make_int4(seg_tile0[s], R, seg_kp[s] | (nt << 16) | (last << 24), (int)(seg_off[s] >> 7));
     }
 }
 
@@ -723,20 +740,29 @@ int mf_build_tiles(mf_matrix_s *A, cudaStream_t s)
     MF_TRY(mf_scan_i64_to_i64(d_cost, A->d_row_cost, tilem, s));
     // seg_tile0[nseg] = tilenum (end sentinel)
     MF_CUDA_TRY(cudaMemcpyAsync(A->d_seg_tile0 + nseg, A->d_tile_ptr + tilem, sizeof(int), cudaMemcpyDeviceToDevice, s));
+    MF_TRY(dalloc(&A->d_seg_hdr, nseg + 1, s));
+    MF_CUDA_TRY(cudaMemsetAsync(A->d_seg_hdr, 0, (size_t)(nseg + 1) * sizeof(int4), s));
+    if (tilem > 0) {
+        k_seg_hdr<<<(tilem + 255) / 256, 256, 0, s>>>(A->d_seg_ptr, A->d_seg_tile0, A->d_seg_kp, A->d_seg_off,
+                                                      tilem, A->d_seg_hdr);
+        MF_CUDA_TRY(cudaGetLastError());
+    }
     long long ent = 0;
     MF_CUDA_TRY(cudaMemcpyAsync(&ent, A->d_seg_off + nseg, sizeof(long long), cudaMemcpyDeviceToHost, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
     A->slice_entries = ent;
+    if ((ent >> 7) >= (1LL << 31)) return MF_ERR_UNSUPPORTED;
     MF_TRY(dalloc(&A->d_meta, ent, s));
     MF_TRY(dalloc(&A->d_v64, ent, s));
     MF_TRY(dalloc(&A->d_v32, ent, s));
     MF_TRY(dalloc(&A->d_v16, ent, s));
     MF_TRY(dalloc(&A->d_v8, ent, s));
+    MF_TRY(dalloc(&A->d_v8ref, ent, s));
     if (tilem > 0 && nseg > 0) {
         k_seg_fill<<<wgrid, kThreads, 0, s>>>(A->d_tile_ptr, A->d_seg_ptr, A->d_seg_kp, A->d_seg_off,
                                               A->d_csr_offset, A->d_csrptr_offset, A->d_tptr, A->d_tcol, A->d_tval,
-                                              A->d_tval_low, A->d_val_i8, tilem, rowA, A->d_meta, A->d_v64,
-                                              A->d_v32, A->d_v16, A->d_v8);
+                                              A->d_tval_low, A->d_val_i8, A->d_val_i8_ref, tilem, rowA, A->d_meta,
+                                              A->d_v64, A->d_v32, A->d_v16, A->d_v8, A->d_v8ref);
         MF_CUDA_TRY(cudaGetLastError());
     }
     MF_CUDA_TRY(cudaStreamSynchronize(s));

@@ -38,6 +38,7 @@ EXPORT_DTYPES = {
     "colstart": np.int32, "colstop": np.int32, "val_f16": np.uint16, "val_i8_ref": np.int8,
     "val_i8": np.int8, "i8_scale": np.float32, "tile_caps": np.uint8, "seg_ptr": np.int32,
     "seg_kp": np.int32, "seg_rowlen": np.uint16, "seg_off": np.int64, "meta": np.uint8, "v64": np.float64,
+    "v32": np.float32, "seg_hdr": np.int32,
 }
 
 

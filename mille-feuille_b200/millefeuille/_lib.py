@@ -28,7 +28,7 @@ class Options(C.Structure):
                 ("fixed_iters", C.c_int), ("replace_every", C.c_int), ("demote_fp16", C.c_double),
                 ("demote_int8", C.c_double), ("use_lossless", C.c_int), ("wait_timeout_s", C.c_double),
                 ("blocks_per_sm", C.c_int), ("threads_per_block", C.c_int), ("x0_given", C.c_int),
-                ("test_stall_barrier", C.c_int)]
+                ("l2_window", C.c_int), ("test_stall_barrier", C.c_int)]
 
 
 class Report(C.Structure):
@@ -36,12 +36,14 @@ class Report(C.Structure):
                 ("relres_true", C.c_double), ("relres_rec", C.c_double), ("residual", C.c_double),
                 ("time_ms", C.c_double), ("replacements", C.c_int), ("grid_blocks", C.c_int),
                 ("threads_per_block", C.c_int), ("tile_uses", C.c_longlong * 4), ("tiles_skipped", C.c_longlong),
-                ("nnz_uses", C.c_longlong * 4)]
+                ("nnz_uses", C.c_longlong * 4), ("phase_ms", C.c_double * 6)]
 
     def as_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("tile_uses", "nnz_uses")}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("tile_uses", "nnz_uses", "phase_ms")}
         d["tile_uses"] = list(self.tile_uses)
         d["nnz_uses"] = list(self.nnz_uses)
+        d["phase_ms"] = dict(zip(("spmv", "vec_update", "dir_update", "barrier", "replacement", "barrier_spin"),
+                                 [round(v, 4) for v in self.phase_ms]))
         return d
 
 
