@@ -87,7 +87,7 @@ void free_matrix(mf_matrix_s *A)
                     A->d_nonzero_row_new, A->d_tile_rowidx, A->d_block_signal, A->d_blockrowid_new,
                     A->d_blockcsr_ptr_new, A->d_rb_idx, A->d_rb_start, A->d_rb_stop, A->d_val_f16,
                     A->d_val_i8_ref, A->d_val_i8, A->d_i8_scale, A->d_tile_caps, A->d_seg_ptr, A->d_seg_tile0,
-                    A->d_seg_off, A->d_seg_hdr, A->d_seg_kp, A->d_seg_rowlen, A->d_meta, A->d_v64, A->d_v32, A->d_v16,
+                    A->d_seg_off, A->d_seg_hdr, A->d_seg_tile, A->d_seg_kp, A->d_seg_rowlen, A->d_meta, A->d_v64, A->d_v32, A->d_v16,
                     A->d_v8, A->d_v8ref, A->d_row_cost};
     for (void *p : ptrs)
         if (p) cudaFree(p);

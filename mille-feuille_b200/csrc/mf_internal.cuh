@@ -71,6 +71,7 @@ struct mf_matrix_s {
     int *d_seg_tile0;          // [nseg+1] first tile of each segment (+ end)
     long long *d_seg_off;      // [nseg+1] entry offset
     int4 *d_seg_hdr;           // [nseg+1] {first tile, tile-row, kp | ntiles << 16 | last << 24, offset / 128}
+    int *d_seg_tile;           // [nseg*16] tile words: column-tile << 8 | caps (0 past the slice's tiles)
     int *d_seg_kp;             // [nseg]
     uint16_t *d_seg_rowlen;    // [nseg*16]
     long long slice_entries;
@@ -126,9 +127,38 @@ __device__ __forceinline__ unsigned int mf_ld_acquire_u32(const unsigned int *p)
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+__device__ __forceinline__ unsigned int mf_ld_relaxed_u32(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ void mf_red_release_add_u32(unsigned int *p, unsigned int v)
 {
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void mf_red_relaxed_add_u32(unsigned int *p, unsigned int v)
+{
+    asm volatile("red.relaxed.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// 16-byte release store / acquire load (two 64-bit words) at gpu scope
+__device__ __forceinline__ void mf_st_release_v2(unsigned long long *p, unsigned long long a, unsigned long long b)
+{
+    asm volatile("st.release.gpu.global.v2.b64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+__device__ __forceinline__ void mf_st_relaxed_v2(unsigned long long *p, unsigned long long a, unsigned long long b)
+{
+    asm volatile("st.relaxed.gpu.global.v2.b64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+__device__ __forceinline__ void mf_ld_acquire_v2(const unsigned long long *p, unsigned long long &a,
+                                                 unsigned long long &b)
+{
+    asm volatile("ld.acquire.gpu.global.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+__device__ __forceinline__ void mf_ld_relaxed_v2(const unsigned long long *p, unsigned long long &a,
+                                                 unsigned long long &b)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
 }
 __device__ __forceinline__ unsigned long long mf_globaltimer()
 {

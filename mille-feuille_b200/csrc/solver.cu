@@ -7,12 +7,12 @@
 //  * a half-warp owns a contiguous range of tile-rows (lane i = row 16R+i) for
 //    every phase, so y rows are written by their owner only (no y atomics) and
 //    every dot product is reduced in a fixed order (deterministic);
-//  * the tile SpMV walks the half-warp's solver slices as a software pipeline:
-//    one 16-byte header per slice, the slice's tile table held one tile per
-//    lane (read with __shfl_sync), the next slice's header / tiles / index bytes
-//    prefetched while the current slice's eight value + x loads are in flight;
-//  * the grid barrier is a monotone counter: red.release.gpu arrive, polled with
-//    ld.acquire.gpu, every wait bounded by %globaltimer (MF_ERR_TIMEOUT);
+//  * the tile SpMV walks the half-warp's solver slices: one 16-byte header per
+//    slice, the slice's tile words held one tile per lane (read with
+//    __shfl_sync), the next slice's descriptor loaded while the current slice's
+//    value + x loads are in flight;
+//  * the grid barrier is a monotone counter: fence + relaxed arrive, relaxed
+//    polls, one acquire fence, every wait bounded by %globaltimer (MF_ERR_TIMEOUT);
 //  * dot products: warp shuffle tree -> per-block partial in a fixed slot ->
 //    after the barrier each block sums the partials in the same order;
 //  * matrix payload is streamed with evict-first loads so the vectors stay in L2.
@@ -43,6 +43,7 @@ struct SolverParams {
     const __half *v16;
     const int8_t *v8, *v8ref;
     const int *tile_col;
+    const int *seg_tile;          // [nseg*16] tile words: column-tile << 8 | caps
     const int *tile_off;          // csr_offset: tile payload offsets (tile nnz for the counters)
     const float *i8_scale;
     const unsigned char *tile_caps;
@@ -82,13 +83,16 @@ __device__ bool grid_barrier(const SolverParams &P, unsigned &epoch, Shared &sh)
     if (threadIdx.x == 0) {
         const unsigned long long tw0 = mf_globaltimer();
         const unsigned target = epoch * gridDim.x + ((P.stall_first_barrier && epoch == 1) ? 1u : 0u);
+        // fence-release pattern: the block's writes (ordered before by bar.sync) are
+        // visible at gpu scope before the arrival; polls are relaxed loads and one
+        // acquire fence follows (an acquire load per poll costs like a fence)
         __threadfence();
-        mf_red_release_add_u32(P.bar, 1u);
+        mf_red_relaxed_add_u32(P.bar, 1u);
         bool ok = true;
         const unsigned long long t0 = mf_globaltimer();
         unsigned spins = 0;
         for (;;) {
-            unsigned v = mf_ld_acquire_u32(P.bar);
+            unsigned v = mf_ld_relaxed_u32(P.bar);
             if ((int)(v - target) >= 0) break;
             if (*(volatile int *)P.err) { ok = false; break; }
             if ((++spins & 63u) == 0u && mf_globaltimer() - t0 > P.timeout_ns) {
@@ -97,7 +101,7 @@ __device__ bool grid_barrier(const SolverParams &P, unsigned &epoch, Shared &sh)
                 break;
             }
         }
-        __threadfence();
+        mf_fence_acq_rel_gpu();
         sh.flag = ok ? 1 : 0;
         if (blockIdx.x == 0 && P.phase_ns) P.phase_ns[5] += mf_globaltimer() - tw0;   // block 0 spin time
     }
@@ -189,8 +193,7 @@ struct XVec {
 // Tile table of a slice, one tile per lane (lane i holds slot i).
 struct TileReg {
     int xb;       // column-tile * 16
-    int pr;       // entry precision
-    float sc;     // int8 scale
+    int pr;       // entry precision of the tile (the slice runs at the half's minimum)
 };
 
 __device__ __forceinline__ int hdr_kp(int4 h) { return h.z & 0xFFFF; }
@@ -198,90 +201,90 @@ __device__ __forceinline__ int hdr_nt(int4 h) { return (h.z >> 16) & 0xFF; }
 __device__ __forceinline__ bool hdr_last(int4 h) { return (h.z >> 24) & 1; }
 __device__ __forceinline__ long long hdr_off(int4 h) { return (long long)h.w << 7; }
 
+// The precision statistic of lane i's tile (tile word tw = column-tile << 8 |
+// caps): the column segment's magnitude (mixed mode) or its reference label
+// (parity mode).  Issued one slice ahead so its latency overlaps a slice.
 template <int MODE, bool F64>
-__device__ __forceinline__ TileReg load_tiles(const SolverParams &P, int4 h, int i, const XVec &X,
-                                              unsigned *cnt)
+__device__ __forceinline__ float load_stat(const XVec &X, int tw, int i, int nt)
 {
-    TileReg T;
-    T.xb = 0;
-    T.pr = MF_P64;
-    T.sc = 0.0f;
-    const int nt = hdr_nt(h);
-    if (i < nt) {
-        const int t = h.x + i;
-        const int jc = P.tile_col[t];
-        T.xb = jc * MF_BS;
-        int pr;
-        if (F64 || MODE == MODE_FP64) {
-            pr = MF_P64;
-        } else if (X.force_pr >= 0) {
-            pr = X.force_pr;
-        } else if (MODE == MODE_MIXED) {
-            const unsigned cap = P.tile_caps[t];
-            const float rel = X.mag[jc] * X.invM;
-            pr = MF_P32;
-            if (rel <= P.demote8) pr = MF_P8;
-            else if (rel <= P.demote16 && (cap & MF_CAP_FP16_OK)) pr = MF_P16;
-            if (P.use_lossless) {
-                if (cap & MF_CAP_EXACT_I8) pr = MF_P8;
-                else if ((cap & MF_CAP_EXACT_F16) && pr == MF_P32) pr = MF_P16;
-            }
-            if (pr == MF_P8) T.sc = P.i8_scale[t];
-        } else {
-            pr = parity_prec(X.lab[jc]);
-        }
-        T.pr = pr;
-        if (cnt) {
-            // shared per-warp counters; a warp's counts stay far below 2^32 per solve
-            atomicAdd(&cnt[pr], 1u);                                            // tile products
-            atomicAdd(&cnt[5 + pr], (unsigned)(P.tile_off[t + 1] - P.tile_off[t]));  // entries
-        }
+    if (F64 || MODE == MODE_FP64 || i >= nt || X.force_pr >= 0) return 0.0f;
+    const int jc = tw >> 8;
+    if (MODE == MODE_MIXED) return X.mag[jc];
+    return (float)X.lab[jc];
+}
+
+// Entry precision of lane i's tile from its tile word and statistic.
+template <int MODE, bool F64>
+__device__ __forceinline__ int tile_prec(const SolverParams &P, int tw, float st, const XVec &X)
+{
+    if (F64 || MODE == MODE_FP64) return MF_P64;
+    if (X.force_pr >= 0) return X.force_pr;
+    if (MODE == MODE_PARITY) return parity_prec((int)st);
+    const unsigned cap = (unsigned)tw & 0xFFu;
+    const float rel = st * X.invM;
+    int pr = MF_P32;
+    if (rel <= P.demote8) pr = MF_P8;
+    else if (rel <= P.demote16 && (cap & MF_CAP_FP16_OK)) pr = MF_P16;
+    if (P.use_lossless) {
+        if (cap & MF_CAP_EXACT_I8) pr = MF_P8;
+        else if ((cap & MF_CAP_EXACT_F16) && pr == MF_P32) pr = MF_P16;
     }
-    return T;
+    return pr;
 }
 
 // Uniform-precision chunk loop: every entry of the slice uses precision PR
 // (FP64 values with FP64 x; otherwise FP32 x, FP32 products and an FP32
 // partial sum per 8-entry chunk, added to the FP64 row sum).
-template <int PR>
-__device__ __forceinline__ double slice_dot_uniform(const SolverParams &P, long long off, int kp, int i,
-                                                    unsigned hmask, int len, const TileReg &T, const XVec &X)
+// A slice is kp/8 chunks of 16 rows x 8 entries.  Per chunk the value loads
+// are issued first (they need only the offset and the row length, both known
+// at the top of the slice), then the index word, then the gathered x; pre()
+// issues the next slice's dependent loads once the first chunk is in flight.
+template <int PR, typename Pre>
+__device__ __forceinline__ double slice_dot_uniform(const SolverParams &P, int4 h, long long off, int i,
+                                                    unsigned hmask, int len, const TileReg &T,
+                                                    const XVec &X, Pre &pre)
 {
+    const int kp = hdr_kp(h);
     const unsigned long long *mrow = (const unsigned long long *)(P.meta + off + (long long)i * kp);
+    float sc = 0.0f;
+    if (PR == MF_P8) sc = (i < hdr_nt(h)) ? P.i8_scale[h.x + i] : 0.0f;
     double acc = 0.0;
     for (int k0 = 0; k0 < kp; k0 += 8) {
-        const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
         if (PR == MF_P64) {
             double v[8], xv[8];
 #pragma unroll
+            for (int j = 0; j < 8; j++)
+                v[j] = (k0 + j < len) ? __ldcs(P.v64 + off + (long long)(k0 + j) * MF_BS + i) : 0.0;
+            const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
+#pragma unroll
             for (int j = 0; j < 8; j++) {
-                const int k = k0 + j;
-                const bool act = k < len;
                 const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
                 const int xi = __shfl_sync(hmask, T.xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
-                const long long e = off + (long long)k * MF_BS + i;
-                v[j] = act ? __ldcs(P.v64 + e) : 0.0;
-                xv[j] = act ? X.x64[xi] : 0.0;
+                xv[j] = (k0 + j < len) ? X.x64[xi] : 0.0;
             }
+            if (k0 == 0) pre();
 #pragma unroll
             for (int j = 0; j < 8; j++) acc = fma(v[j], xv[j], acc);
         } else {
             float v[8], xv[8];
 #pragma unroll
             for (int j = 0; j < 8; j++) {
-                const int k = k0 + j;
-                const bool act = k < len;
+                const long long e = off + (long long)(k0 + j) * MF_BS + i;
+                const bool act = k0 + j < len;
+                if (PR == MF_P32) v[j] = act ? __ldcs(P.v32 + e) : 0.0f;
+                else if (PR == MF_P16) v[j] = act ? __half2float(P.v16[e]) : 0.0f;
+                else v[j] = act ? (float)P.v8[e] : 0.0f;
+            }
+            const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
                 const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
                 const int slot = (int)(mm >> 4);
                 const int xi = __shfl_sync(hmask, T.xb, slot, 16) + (int)(mm & 15u);
-                const long long e = off + (long long)k * MF_BS + i;
-                float fv;
-                if (PR == MF_P32) fv = act ? __ldcs(P.v32 + e) : 0.0f;
-                else if (PR == MF_P16) fv = act ? __half2float(P.v16[e]) : 0.0f;
-                else fv = act ? (float)P.v8[e] * __shfl_sync(hmask, T.sc, slot, 16) : 0.0f;
-                v[j] = fv;
-                xv[j] = act ? X.x32[xi] : 0.0f;
+                xv[j] = (k0 + j < len) ? X.x32[xi] : 0.0f;
+                if (PR == MF_P8) v[j] *= __shfl_sync(hmask, sc, slot, 16);
             }
+            if (k0 == 0) pre();
             float part = 0.0f;
 #pragma unroll
             for (int j = 0; j < 8; j++) part = fmaf(v[j], xv[j], part);
@@ -297,21 +300,29 @@ __device__ __forceinline__ double slice_dot_uniform(const SolverParams &P, long 
 // the HBM copy bandwidth, where a software-pipelined variant with twice the
 // registers per thread did not.  In mixed mode a slice runs in one precision,
 // the most conservative of its tiles' labels (no per-entry dispatch).
-template <int MODE, bool F64>
+template <int MODE, bool F64, typename Pre>
 __device__ __forceinline__ double slice_dot(const SolverParams &P, int4 h, int i, unsigned hmask, int len,
-                                            const TileReg &T, const XVec &X)
+                                            long long off, const TileReg &T, const XVec &X,
+                                            unsigned *cnt, Pre &pre)
 {
-    const int kp = hdr_kp(h);
-    const long long off = hdr_off(h);
-    if (MODE == MODE_FP64 || F64) return slice_dot_uniform<MF_P64>(P, off, kp, i, hmask, len, T, X);
     // precision codes order FP64 < FP32 < FP16 < INT8: the minimum is the most precise
-    int pr = (i < hdr_nt(h)) ? T.pr : MF_P8;
+    int pr = MF_P64;
+    if (!(MODE == MODE_FP64 || F64)) {
+        pr = (i < hdr_nt(h)) ? T.pr : MF_P8;
 #pragma unroll
-    for (int o = 8; o; o >>= 1) pr = min(pr, __shfl_xor_sync(hmask, pr, o));
-    if (pr == MF_P32) return slice_dot_uniform<MF_P32>(P, off, kp, i, hmask, len, T, X);
-    if (pr == MF_P64) return slice_dot_uniform<MF_P64>(P, off, kp, i, hmask, len, T, X);
-    if (pr == MF_P16) return slice_dot_uniform<MF_P16>(P, off, kp, i, hmask, len, T, X);
-    return slice_dot_uniform<MF_P8>(P, off, kp, i, hmask, len, T, X);
+        for (int o = 8; o; o >>= 1) pr = min(pr, __shfl_xor_sync(hmask, pr, o));
+    }
+    if (cnt) {
+        // shared per-warp counters of the executed precision; a warp's counts
+        // stay far below 2^32 per solve
+        if (i < hdr_nt(h)) atomicAdd(&cnt[pr], 1u);    // tile products
+        if (len) atomicAdd(&cnt[5 + pr], (unsigned)len);  // entries
+    }
+    if (MODE == MODE_FP64 || F64) return slice_dot_uniform<MF_P64>(P, h, off, i, hmask, len, T, X, pre);
+    if (pr == MF_P32) return slice_dot_uniform<MF_P32>(P, h, off, i, hmask, len, T, X, pre);
+    if (pr == MF_P64) return slice_dot_uniform<MF_P64>(P, h, off, i, hmask, len, T, X, pre);
+    if (pr == MF_P16) return slice_dot_uniform<MF_P16>(P, h, off, i, hmask, len, T, X, pre);
+    return slice_dot_uniform<MF_P8>(P, h, off, i, hmask, len, T, X, pre);
 }
 
 // Parity mode: the reference's tile arithmetic (main-cg-mixed.cu:1130-1214):
@@ -374,21 +385,61 @@ __device__ __forceinline__ double slice_dot_parity(const SolverParams &P, int4 h
 // y = A x over the half-warp's slices [sb, se); epi(R, y) is called once per
 // tile-row (after its last slice) with the row sum of lane i.
 // F64: every tile in FP64 (the FP64 residual replacement and the FP64 SpMV).
+//
+// Descriptor pipeline: a half-warp's slices are stored back to back, so slice
+// s+1 starts where slice s ends (offset + 16 * kp).  The words indexed by the
+// slice number alone (header, lane i's tile word and row length) are loaded one
+// slice ahead, at the top of the previous slice, together with that slice's own
+// loads; the precision statistic (mixed / parity) is loaded one slice ahead
+// once the tile word is in.  A slice then waits for two round trips: values +
+// index word, then the gathered x.
 template <int MODE, bool F64, typename Epi>
 __device__ __forceinline__ void spmv_range(const SolverParams &P, int sb, int se, int i, unsigned hmask,
                                            const XVec &X, unsigned *cnt, Epi epi)
 {
+    if (sb >= se) return;
+    int4 h = P.seg_hdr[sb];
+    int tw = P.seg_tile[(long long)sb * MF_BS + i];
+    int len = P.seg_rowlen[(long long)sb * MF_BS + i];
+    float st = load_stat<MODE, F64>(X, tw, i, hdr_nt(h));
+    long long off = hdr_off(h);
     double acc = 0.0;
     for (int s = sb; s < se; s++) {
-        const int4 h = P.seg_hdr[s];
-        const TileReg T = load_tiles<MODE, F64>(P, h, i, X, cnt);
-        const int len = P.seg_rowlen[(long long)s * MF_BS + i];
-        if (MODE == MODE_PARITY && !F64) acc += slice_dot_parity(P, h, i, hmask, len, T, X);
-        else acc += slice_dot<MODE, F64>(P, h, i, hmask, len, T, X);
+        const bool more = s + 1 < se;
+        int4 hn = make_int4(0, 0, 0, 0);
+        int twn = 0, lenn = 0;
+        if (more) {
+            hn = P.seg_hdr[s + 1];
+            twn = P.seg_tile[(long long)(s + 1) * MF_BS + i];
+            lenn = P.seg_rowlen[(long long)(s + 1) * MF_BS + i];
+        }
+        float stn = 0.0f;
+        auto pre = [&]() {
+            if (more) stn = load_stat<MODE, F64>(X, twn, i, hdr_nt(hn));
+        };
+        TileReg T;
+        T.xb = (tw >> 8) * MF_BS;
+        T.pr = tile_prec<MODE, F64>(P, tw, st, X);
+        if (MODE == MODE_PARITY && !F64) {
+            pre();
+            if (cnt && i < hdr_nt(h)) {
+                const int t = h.x + i;
+                atomicAdd(&cnt[T.pr], 1u);
+                atomicAdd(&cnt[5 + T.pr], (unsigned)(P.tile_off[t + 1] - P.tile_off[t]));
+            }
+            acc += slice_dot_parity(P, h, i, hmask, len, T, X);
+        } else {
+            acc += slice_dot<MODE, F64>(P, h, i, hmask, len, off, T, X, cnt, pre);
+        }
         if (hdr_last(h)) {
             epi(h.y, acc);
             acc = 0.0;
         }
+        off += (long long)hdr_kp(h) * MF_BS;
+        h = hn;
+        tw = twn;
+        len = lenn;
+        st = stn;
     }
 }
 
@@ -1000,6 +1051,7 @@ void fill_params(SolverParams &P, mf_matrix_s *A, Workspace *w)
     P.v8 = A->d_v8;
     P.v8ref = A->d_v8ref;
     P.tile_col = A->d_tile_columnidx;
+    P.seg_tile = A->d_seg_tile;
     P.tile_off = A->d_csr_offset;
     P.i8_scale = A->d_i8_scale;
     P.tile_caps = A->d_tile_caps;

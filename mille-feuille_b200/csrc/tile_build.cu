@@ -515,16 +515,23 @@ __global__ void k_seg_fill(const int *__restrict__ tile_ptr, const int *__restri
 // Packed per-segment header read once per segment by the solver's pipeline:
 // {first tile, tile-row, Kp | ntiles << 16 | last-slice-of-tile-row << 24,
 // entry offset / 128} (offsets are multiples of 128: Kp is a multiple of 8, 16 rows).
+// Also writes the slice's tile words at a fixed stride of 16 per slice
+// (column-tile << 8 | capability bits, 0 past the slice's tiles), so the solver
+// can fetch them by slice number without waiting for the header.
 __global__ void k_seg_hdr(const int *__restrict__ seg_ptr, const int *__restrict__ seg_tile0,
-                          const int *__restrict__ seg_kp, const long long *__restrict__ seg_off, int tilem,
-                          int4 *__restrict__ hdr)
+                          const int *__restrict__ seg_kp, const long long *__restrict__ seg_off,
+                          const int *__restrict__ tile_columnidx, const unsigned char *__restrict__ caps, int tilem,
+                          int4 *__restrict__ hdr, int *__restrict__ seg_tile)
 {
     int R = blockIdx.x * blockDim.x + threadIdx.x;
     if (R >= tilem) return;
     for (int s = seg_ptr[R]; s < seg_ptr[R + 1]; s++) {
-        const int nt = seg_tile0[s + 1] - seg_tile0[s];
+        const int t0 = seg_tile0[s];
+        const int nt = seg_tile0[s + 1] - t0;
         const int last = (s + 1 == seg_ptr[R + 1]) ? 1 : 0;     // last slice of its tile-row
-        hdr[s] = make_int4(seg_tile0[s], R, seg_kp[s] | (nt << 16) | (last << 24), (int)(seg_off[s] >> 7));
+        hdr[s] = make_int4(t0, R, seg_kp[s] | (nt << 16) | (last << 24), (int)(seg_off[s] >> 7));
+        for (int i = 0; i < MF_BS; i++)
+            seg_tile[(long long)s * MF_BS + i] = (i < nt) ? ((tile_columnidx[t0 + i] << 8) | caps[t0 + i]) : 0;
     }
 }
 
@@ -742,9 +749,12 @@ int mf_build_tiles(mf_matrix_s *A, cudaStream_t s)
     MF_CUDA_TRY(cudaMemcpyAsync(A->d_seg_tile0 + nseg, A->d_tile_ptr + tilem, sizeof(int), cudaMemcpyDeviceToDevice, s));
     MF_TRY(dalloc(&A->d_seg_hdr, nseg + 1, s));
     MF_CUDA_TRY(cudaMemsetAsync(A->d_seg_hdr, 0, (size_t)(nseg + 1) * sizeof(int4), s));
+    MF_TRY(dalloc(&A->d_seg_tile, ((long long)nseg + 1) * MF_BS, s));
+    if ((long long)A->tilen >= (1LL << 23)) return MF_ERR_UNSUPPORTED;   // column tile must fit 23 bits
     if (tilem > 0) {
         k_seg_hdr<<<(tilem + 255) / 256, 256, 0, s>>>(A->d_seg_ptr, A->d_seg_tile0, A->d_seg_kp, A->d_seg_off,
-                                                      tilem, A->d_seg_hdr);
+                                                      A->d_tile_columnidx, A->d_tile_caps, tilem, A->d_seg_hdr,
+                                                      A->d_seg_tile);
         MF_CUDA_TRY(cudaGetLastError());
     }
     long long ent = 0;
