@@ -29,6 +29,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kRedKinds = 10;     // reduction slot groups
 constexpr int kRedWidth = 4;      // doubles per group per block
 constexpr int kDefaultLB = 2;     // default register-budget variant of the persistent kernel
+constexpr int kVB = 4;            // tile-rows per step in the vector phases (loads in flight)
 
 enum { MODE_FP64 = 0, MODE_MIXED = 1, MODE_PARITY = 2 };
 
@@ -51,6 +52,7 @@ struct SolverParams {
     const double *b;
     double *x, *r, *p, *q, *rh, *s, *t;
     float *p32, *s32, *mag_p, *mag_s;
+    float *r32, *mag_r;           // CG with the SpMV on r: r's FP32 shadow / segment magnitudes
     __half *p16, *s16;
     int8_t *p8, *s8;
     signed char *lab_p, *lab_s;
@@ -71,7 +73,7 @@ struct Shared {
     double wred[kWarps][kRedWidth];
     double bcast[kRedWidth];
     int flag;
-    unsigned cnt[kWarps][10];   // per-warp tile / entry counters (tile products per precision)
+    unsigned cnt[kWarps * 2][10];   // per-half-warp tile / entry counters per precision (mixed / parity)
     unsigned long long clk_t, clk_acc[5];   // block 0 phase clock
 };
 
@@ -313,10 +315,16 @@ __device__ __forceinline__ double slice_dot(const SolverParams &P, int4 h, int i
         for (int o = 8; o; o >>= 1) pr = min(pr, __shfl_xor_sync(hmask, pr, o));
     }
     if (cnt) {
-        // shared per-warp counters of the executed precision; a warp's counts
+        // the half-warp's own counter slots (lane 0 writes, no atomics): tile
+        // products and entries of the executed precision; a half-warp's counts
         // stay far below 2^32 per solve
-        if (i < hdr_nt(h)) atomicAdd(&cnt[pr], 1u);    // tile products
-        if (len) atomicAdd(&cnt[5 + pr], (unsigned)len);  // entries
+        int sl = len;
+#pragma unroll
+        for (int o = 8; o; o >>= 1) sl += __shfl_xor_sync(hmask, sl, o);
+        if (i == 0) {
+            cnt[pr] += (unsigned)hdr_nt(h);
+            cnt[5 + pr] += (unsigned)sl;
+        }
     }
     if (MODE == MODE_FP64 || F64) return slice_dot_uniform<MF_P64>(P, h, off, i, hmask, len, T, X, pre);
     if (pr == MF_P32) return slice_dot_uniform<MF_P32>(P, h, off, i, hmask, len, T, X, pre);
@@ -513,7 +521,7 @@ __device__ __forceinline__ void publish_dir(int R, int row, bool valid, double v
                                             __half *v16, int8_t *v8, float *mag, signed char *lab, float &bmax,
                                             unsigned hmask, bool labels)
 {
-    if (valid) v32[row] = (float)vnew;
+    if (MODE != MODE_FP64 && valid) v32[row] = (float)vnew;
     if (MODE == MODE_MIXED) {
         float m = half_max(valid ? (float)fabs(vnew) : 0.0f, hmask);
         bmax = fmaxf(bmax, m);
@@ -585,8 +593,11 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     __shared__ Shared sh;
     const Ctx c = make_ctx(P);
     unsigned epoch = 0;
-    unsigned *cnt = sh.cnt[c.wib];
-    if (c.lane < 10) cnt[c.lane] = 0u;
+    // tile-use counters: FP64 mode needs none (every tile of every SpMV is FP64;
+    // the host derives the totals from the SpMV count)
+    unsigned *cnt = (MODE == MODE_FP64) ? nullptr : sh.cnt[c.wib * 2 + c.half];
+    if (cnt && c.i < 10) cnt[c.i] = 0u;
+    int nspmv = 0;
     __syncwarp();
     PhaseClock clk;
     clk.start(&sh);
@@ -624,7 +635,142 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     double rr_true = rr;
     if (!P.fixed_iters && rr <= thr2) { conv = 1; last_true = 1; }
 
+    // tile-rows without slices (all-zero rows) get no SpMV epilogue
+    bool has_empty = false;
+    for (int R = c.rbeg; R < c.rend && !has_empty; R++) has_empty = P.seg_ptr[R] == P.seg_ptr[R + 1];
+    double beta2 = 0.0;
+
     while (!conv && k < P.max_iter) {
+        if (MODE != MODE_PARITY && !bicg) {
+            // CG with two grid syncs per iteration.  The SpMV is applied to r:
+            // w = A r, then p = r + beta p and q = A p = w + beta q, so p never
+            // needs a halo of its own; alpha = r.r / p.q and beta = r'.r' / r.r
+            // are the textbook CG scalars (main-cg-mixed.cu:1224-1382 keeps the
+            // same formulas with the SpMV on p and a third sync).
+            // ---- A: w = A r; p = r + beta p; q = w + beta q; p.q ----
+            double ppq = 0.0;
+            spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
+                                    make_x(P.r, P.r32, nullptr, nullptr, P.mag_r, nullptr, invM), cnt,
+                                    [&](int R, double y) {
+                                        const int row = R * MF_BS + c.i;
+                                        if (row < n) {
+                                            const double pn = P.r[row] + beta2 * P.p[row];
+                                            const double qn = y + beta2 * P.q[row];
+                                            P.p[row] = pn;
+                                            P.q[row] = qn;
+                                            ppq += pn * qn;
+                                        }
+                                    });
+            if (has_empty) {
+                for (int R = c.rbeg; R < c.rend; R++) {
+                    if (P.seg_ptr[R] != P.seg_ptr[R + 1]) continue;
+                    const int row = R * MF_BS + c.i;
+                    if (row < n) {
+                        const double pn = P.r[row] + beta2 * P.p[row];
+                        const double qn = beta2 * P.q[row];
+                        P.p[row] = pn;
+                        P.q[row] = qn;
+                        ppq += pn * qn;
+                    }
+                }
+            }
+            nspmv++;
+            clk.lap(PH_SPMV);
+            block_partial(P, sh, 1, ppq, 0, 0, 0, 1, 0u);
+            if (!grid_barrier(P, epoch, sh)) return;
+            grid_collect(P, sh, 1, 1, 0u, v);
+            clk.lap(PH_BAR);
+            const double alpha2 = rr / v[0];
+            if (!isfinite(alpha2)) { status = MF_ERR_BREAKDOWN; break; }
+            // ---- B: x += alpha p; r -= alpha q; r.r; r's shadow ----
+            double prr = 0.0;
+            float rmax = 0.0f;
+            // kVB tile-rows per step: all loads first, so kVB round trips overlap
+            for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
+                double xv[kVB], pv[kVB], rv[kVB], qv[kVB];
+#pragma unroll
+                for (int u = 0; u < kVB; u++) {
+                    const int row = (R0 + u) * MF_BS + c.i;
+                    const bool valid = R0 + u < c.rend && row < n;
+                    xv[u] = valid ? P.x[row] : 0.0;
+                    pv[u] = valid ? P.p[row] : 0.0;
+                    rv[u] = valid ? P.r[row] : 0.0;
+                    qv[u] = valid ? P.q[row] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kVB; u++) {
+                    const int R = R0 + u;
+                    if (R >= c.rend) break;      // uniform over the half-warp
+                    const int row = R * MF_BS + c.i;
+                    const bool valid = row < n;
+                    const double rn = valid ? rv[u] - alpha2 * qv[u] : 0.0;
+                    if (valid) {
+                        P.x[row] = xv[u] + alpha2 * pv[u];
+                        P.r[row] = rn;
+                        prr += rn * rn;
+                    }
+                    publish_dir<MODE>(R, row, valid, rn, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
+                                      c.hmask, false);
+                }
+            }
+            clk.lap(PH_VECB);
+            block_partial(P, sh, 2, prr, (double)rmax, 0, 0, 2, 0x2u);
+            if (!grid_barrier(P, epoch, sh)) return;
+            grid_collect(P, sh, 2, 2, 0x2u, v);
+            clk.lap(PH_BAR);
+            double rr_new = v[0];
+            invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
+            k++;
+            last_true = 0;
+            const bool want_check = !P.fixed_iters && rr_new <= thr2;
+            const bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
+            if (want_check || want_repl) {
+                // ---- FP64 true residual r = b - A x (x is current), r's shadow ----
+                double prt = 0.0;
+                rmax = 0.0f;
+                spmv_range<MODE, true>(P, c.sbeg, c.send, c.i, c.hmask, fp64_x(P.x), nullptr,
+                                       [&](int R, double y) {
+                                           const int row = R * MF_BS + c.i;
+                                           const bool valid = row < n;
+                                           double rv = 0.0;
+                                           if (valid) {
+                                               rv = P.b[row] - y;
+                                               P.r[row] = rv;
+                                               prt += rv * rv;
+                                           }
+                                           publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr,
+                                                             P.mag_r, nullptr, rmax, c.hmask, false);
+                                       });
+                if (has_empty) {
+                    for (int R = c.rbeg; R < c.rend; R++) {
+                        if (P.seg_ptr[R] != P.seg_ptr[R + 1]) continue;
+                        const int row = R * MF_BS + c.i;
+                        const bool valid = row < n;
+                        const double rv = valid ? P.b[row] : 0.0;
+                        if (valid) {
+                            P.r[row] = rv;
+                            prt += rv * rv;
+                        }
+                        publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
+                                          c.hmask, false);
+                    }
+                }
+                clk.lap(PH_REPL);
+                block_partial(P, sh, 5, prt, (double)rmax, 0, 0, 2, 0x2u);
+                if (!grid_barrier(P, epoch, sh)) return;
+                grid_collect(P, sh, 5, 2, 0x2u, v);
+                clk.lap(PH_BAR);
+                rr_new = v[0];
+                invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
+                rr_true = rr_new;
+                repl++;
+                last_true = 1;
+                if (!P.fixed_iters && rr_new <= thr2) { rr = rr_new; conv = 1; break; }
+            }
+            beta2 = rr_new / rr;
+            rr = rr_new;
+            continue;
+        }
         double alpha = 0.0, omega = 0.0;
         if (!bicg) {
             // ---- A: q = A p, p.q ----
@@ -638,6 +784,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                                      ppq += P.p[row] * y;
                                  }
                              });
+            nspmv++;
             clk.lap(PH_SPMV);
             block_partial(P, sh, 1, ppq, 0, 0, 0, 1, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
@@ -647,13 +794,23 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             if (!isfinite(alpha)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B: r -= alpha q, r.r  (x is updated with p in phase C) ----
             double prr = 0.0;
-#pragma unroll 4
-            for (int R = c.rbeg; R < c.rend; R++) {
-                const int row = R * MF_BS + c.i;
-                if (row < n) {
-                    const double rv = P.r[row] - alpha * P.q[row];
-                    P.r[row] = rv;
-                    prr += rv * rv;
+            for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
+                double rv[kVB], qv[kVB];
+#pragma unroll
+                for (int u = 0; u < kVB; u++) {
+                    const int row = (R0 + u) * MF_BS + c.i;
+                    const bool valid = R0 + u < c.rend && row < n;
+                    rv[u] = valid ? P.r[row] : 0.0;
+                    qv[u] = valid ? P.q[row] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < kVB; u++) {
+                    const int row = (R0 + u) * MF_BS + c.i;
+                    if (R0 + u < c.rend && row < n) {
+                        const double rn = rv[u] - alpha * qv[u];
+                        P.r[row] = rn;
+                        prr += rn * rn;
+                    }
                 }
             }
             clk.lap(PH_VECB);
@@ -673,6 +830,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                                      prv += P.rh[row] * y;
                                  }
                              });
+            nspmv++;
             clk.lap(PH_SPMV);
             block_partial(P, sh, 1, prv, 0, 0, 0, 1, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
@@ -712,6 +870,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                                      ptt += y * y;
                                  }
                              });
+            nspmv++;
             clk.lap(PH_SPMV);
             block_partial(P, sh, 3, pts, ptt, 0, 0, 2, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
@@ -799,17 +958,31 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
         }
         rr = rr_new;
         bmax = 0.0f;
-        for (int R = c.rbeg; R < c.rend; R++) {
-            const int row = R * MF_BS + c.i;
-            const bool valid = row < n;
-            double pold = 0.0, pn = 0.0;
-            if (valid) {
-                pold = P.p[row];
-                if (!x_done) P.x[row] += alpha * pold;
-                pn = bicg ? P.r[row] + beta * (pold - omega * P.q[row]) : P.r[row] + beta * pold;
-                P.p[row] = pn;
+        for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
+            double pv[kVB], rv[kVB], xq[kVB];    // xq: x (CG, x not yet updated) or v (BiCGSTAB)
+#pragma unroll
+            for (int u = 0; u < kVB; u++) {
+                const int row = (R0 + u) * MF_BS + c.i;
+                const bool valid = R0 + u < c.rend && row < n;
+                pv[u] = valid ? P.p[row] : 0.0;
+                rv[u] = valid ? P.r[row] : 0.0;
+                xq[u] = (valid && (bicg || !x_done)) ? (bicg ? P.q[row] : P.x[row]) : 0.0;
             }
-            publish_dir<MODE>(R, row, valid, pn, pold, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, true);
+#pragma unroll
+            for (int u = 0; u < kVB; u++) {
+                const int R = R0 + u;
+                if (R >= c.rend) break;          // uniform over the half-warp
+                const int row = R * MF_BS + c.i;
+                const bool valid = row < n;
+                const double pold = pv[u];
+                const double pn = bicg ? rv[u] + beta * (pold - omega * xq[u]) : rv[u] + beta * pold;
+                if (valid) {
+                    if (!bicg && !x_done) P.x[row] = xq[u] + alpha * pold;
+                    P.p[row] = pn;
+                }
+                publish_dir<MODE>(R, row, valid, valid ? pn : 0.0, pold, P.p32, P.p16, P.p8, P.mag_p, P.lab_p,
+                                  bmax, c.hmask, true);
+            }
         }
         clk.lap(PH_VECC);
         block_partial(P, sh, 6, (double)bmax, 0, 0, 0, 1, 0x1u);
@@ -841,7 +1014,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     }
     // tile-use counters
     __syncwarp();
-    if (c.lane < 10 && cnt[c.lane]) atomicAdd(&P.counts[c.lane], (unsigned long long)cnt[c.lane]);
+    if (cnt && c.i < 10 && cnt[c.i]) atomicAdd(&P.counts[c.i], (unsigned long long)cnt[c.i]);
     if (clk.on() && P.phase_ns)
         for (int j = 0; j < 5; j++) P.phase_ns[j] = sh.clk_acc[j];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -852,6 +1025,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
         P.out[4] = sqrt(rr);
         P.out[5] = (double)repl;
         P.out[6] = (double)status;
+        P.out[7] = (double)nspmv;
     }
 }
 
@@ -1060,6 +1234,8 @@ void fill_params(SolverParams &P, mf_matrix_s *A, Workspace *w)
         P.x = w->x; P.r = w->r; P.p = w->p; P.q = w->q; P.rh = w->rh; P.s = w->s; P.t = w->t;
         P.p32 = w->p32; P.s32 = w->s32; P.p16 = w->p16; P.s16 = w->s16; P.p8 = w->p8; P.s8 = w->s8;
         P.mag_p = w->mag_p; P.mag_s = w->mag_s; P.lab_p = w->lab_p; P.lab_s = w->lab_s;
+        // CG in the FP64 / mixed modes multiplies r, not p: r's shadow takes p's slots
+        P.r32 = w->p32; P.mag_r = w->mag_p;
         P.red = w->red; P.bar = w->bar; P.err = w->err; P.out = w->out; P.counts = w->counts;
         P.phase_ns = w->phase_ns;
     }
@@ -1221,6 +1397,12 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
         for (int j = 0; j < 4; j++) rep->tile_uses[j] = (long long)counts[j];
         rep->tiles_skipped = (long long)counts[4];
         for (int j = 0; j < 4; j++) rep->nnz_uses[j] = (long long)counts[5 + j];
+        if (mode == MODE_FP64) {
+            // every tile of every SpMV phase runs in FP64: counted here, not in the kernel
+            const long long nspmv = (long long)out[7];
+            rep->tile_uses[0] = nspmv * A->tilenum;
+            rep->nnz_uses[0] = nspmv * A->nnz;
+        }
         for (int j = 0; j < 6; j++) rep->phase_ms[j] = (double)phase[j] * 1e-6;
     }
     if (err) return err;
