@@ -196,12 +196,15 @@ def run_ours(args, rank, world, local_rank):
     peak, peak_kind = _peaks()
     alg = algorithmic_bytes(rep, n, nnz, T)
     achieved = alg / (rep["time_ms"] * 1e-3) / 1e9
+    # DRAM bytes of one launch, from an ncu capture of this same solve (1-pass dram
+    # metrics, committed under profiles/), scaled by iteration count if it differs
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "solve_mixed_poisson3d_traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get("dram_bytes_per_launch")
+                tj = json.load(f)
+            traffic = int(tj["dram_bytes_per_launch"] * rep["iterations"] / tj["iterations"])
         except Exception:
             traffic = None
     # independent FP64 check of the returned solution (host, scipy)
@@ -321,8 +324,12 @@ def run_profile(args):
         print(json.dumps({"profile": kind, "spmv_ms": G.last_spmv_ms}))
         return
     prec = "fp64" if kind == "solve_fp64" else "mixed"
-    o = mf.default_options(precision=prec, tol=TOL, max_iter=args.profile_iters, fixed_iters=1, replace_every=0,
-                           blocks_per_sm=args.blocks_per_sm)
+    if kind == "solve_mixed_tol":
+        # the bench's own solve: to 1e-8 with FP64 residual replacement every 50 iterations
+        o = mf.default_options(precision="mixed", tol=TOL)
+    else:
+        o = mf.default_options(precision=prec, tol=TOL, max_iter=args.profile_iters, fixed_iters=1,
+                               replace_every=0, blocks_per_sm=args.blocks_per_sm)
     for _ in range(2):
         _, rep = G.solve(bd, xd, options=o)
     print(json.dumps({"profile": kind, "iterations": rep["iterations"], "kernel_ms": rep["time_ms"],
@@ -332,7 +339,7 @@ def run_profile(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["solve_fp64", "solve_mixed", "spmv_fp64", "spmv_mixed"],
+    ap.add_argument("--profile", choices=["solve_fp64", "solve_mixed", "solve_mixed_tol", "spmv_fp64", "spmv_mixed"],
                     help="run one small launch of a kernel for an ncu capture and exit")
     ap.add_argument("--profile-iters", type=int, default=20)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
