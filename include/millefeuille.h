@@ -200,6 +200,36 @@ int mf_solve(mf_matrix A, const double *b, double *x, const mf_options *opt, mf_
 int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs,
             void *stream, double *elapsed_ms);
 
+/*
+ * y = A x like mf_spmv, but the call allocates no memory (no cudaMalloc /
+ * cudaFree, no host staging).  No counterpart in the reference: its
+ * entry points allocate and free device memory on every call.  For callers
+ * that must not allocate -- code that runs with the device memory already
+ * handed to another allocator, or inside a latency-critical loop where an
+ * allocation's implicit device synchronisation is not acceptable.
+ *
+ *  - x and y are device pointers (n_cols and n_rows doubles); precision is
+ *    MF_PREC_FP64 or MF_PREC_MIXED (every tile in FP32), as for mf_spmv.
+ *  - The call is asynchronous on `stream` (NULL: default stream); y is ready
+ *    when the stream reaches that point.
+ *  - Scratch: the padded copy of x (and its FP32 shadow) lives in a fixed
+ *    device buffer compiled into the library, MF_SPMV_NOALLOC_MAX_LEN entries
+ *    (16 MB + 8 MB per device).  Matrices whose padded vector length,
+ *    16 * ceil(max(n_rows, n_cols) / 16), exceeds it are rejected with
+ *    MF_ERR_UNSUPPORTED before anything is launched.
+ *  - Nothing has to start at zero: each call writes every scratch entry the
+ *    kernel reads (x, then zeros up to the padded length).
+ *  - The first call on a device looks the buffer up (cudaGetSymbolAddress,
+ *    which may load the library's device code); make that first call before
+ *    any stream capture.  Later calls only issue a memset, a copy and the
+ *    kernel(s).
+ *  - One buffer per device is shared by all handles and threads: calls on
+ *    the same device must not overlap in time (issue them on one stream, or
+ *    order the streams), otherwise they race on the scratch.
+ */
+#define MF_SPMV_NOALLOC_MAX_LEN (1 << 21)
+int mf_spmv_noalloc(mf_matrix A, const double *x, double *y, int precision, void *stream);
+
 /* Test hook: segment labels of the reference rule for (p_old, p_new) device or
  * host arrays of length nseg*16; codes as d_vis (0 FP64, 4 FP32, 3 FP16, 2 INT8,
  * 1 bypass).  Runs the same device classifier the parity-mode solver uses. */

@@ -327,6 +327,13 @@ extern "C" int mf_spmv(mf_matrix A, const double *x, double *y, int precision, i
     return rc;
 }
 
+extern "C" int mf_spmv_noalloc(mf_matrix A, const double *x, double *y, int precision, void *stream)
+{
+    if (!A || !x || !y) return MF_ERR_INVALID;
+    if (precision != MF_PREC_FP64 && precision != MF_PREC_MIXED) return MF_ERR_INVALID;
+    return mf_spmv_noalloc_run(A, x, y, precision, (cudaStream_t)stream);
+}
+
 extern "C" int mf_debug_ref_labels(const double *p_old, const double *p_new, int nseg, int *vis, int device_ptrs)
 {
     if (nseg < 0 || (nseg > 0 && (!p_old || !p_new || !vis))) return MF_ERR_INVALID;

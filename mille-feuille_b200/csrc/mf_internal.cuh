@@ -115,6 +115,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
                   mf_report *rep, cudaStream_t s);
 int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s,
                 double *elapsed_ms);
+int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s);
 int mf_ref_labels_run(const double *d_pold, const double *d_pnew, int nseg, int *d_vis,
                       cudaStream_t s);
 void mf_solver_free_ws(mf_matrix_s *A);

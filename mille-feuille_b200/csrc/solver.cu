@@ -20,6 +20,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace {
@@ -1458,5 +1459,78 @@ int mf_ref_labels_run(const double *d_pold, const double *d_pnew, int nseg, int 
     k_ref_labels<<<(nseg + segs_per_block - 1) / segs_per_block, threads, 0, s>>>(d_pold, d_pnew, nseg, d_vis);
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaStreamSynchronize(s));
+    return MF_SUCCESS;
+}
+
+// ------------------------------------------------------------ allocation-free SpMV
+// Scratch of mf_spmv_noalloc: the padded FP64 copy of x and its FP32 shadow, as
+// file-scope device arrays (allocated with the module, one per device context),
+// so the call itself allocates nothing.
+static __device__ __align__(256) double g_noalloc_x[MF_SPMV_NOALLOC_MAX_LEN];
+static __device__ __align__(256) float g_noalloc_x32[MF_SPMV_NOALLOC_MAX_LEN];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double *g_noalloc_x_addr[kMaxDevices];
+float *g_noalloc_x32_addr[kMaxDevices];
+
+// Device addresses of the scratch arrays on the current device, looked up once
+// per device (cudaGetSymbolAddress; the first lookup may load the module).
+int noalloc_scratch(int dev, double **x, float **x32)
+{
+    if (dev < 0 || dev >= kMaxDevices) return MF_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_x_addr[dev]) {
+        void *px = nullptr, *px32 = nullptr;
+        MF_CUDA_TRY(cudaGetSymbolAddress(&px, g_noalloc_x));
+        MF_CUDA_TRY(cudaGetSymbolAddress(&px32, g_noalloc_x32));
+        g_noalloc_x_addr[dev] = (double *)px;
+        g_noalloc_x32_addr[dev] = (float *)px32;
+    }
+    *x = g_noalloc_x_addr[dev];
+    *x32 = g_noalloc_x32_addr[dev];
+    return MF_SUCCESS;
+}
+}  // namespace
+
+int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s)
+{
+    const long long L = A->vec_len;
+    if (L > MF_SPMV_NOALLOC_MAX_LEN) return MF_ERR_UNSUPPORTED;
+    int dev = 0;
+    MF_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != A->dev) return MF_ERR_INVALID;
+    double *x = nullptr;
+    float *x32 = nullptr;
+    MF_TRY(noalloc_scratch(dev, &x, &x32));
+    // x, then zeros up to the padded length: every entry the kernel reads is written here
+    MF_CUDA_TRY(cudaMemcpyAsync(x, d_x, (size_t)A->n_cols * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (L > A->n_cols)
+        MF_CUDA_TRY(cudaMemsetAsync(x + A->n_cols, 0, (size_t)(L - A->n_cols) * sizeof(double), s));
+    const int fpr = precision == MF_PREC_FP64 ? MF_P64 : MF_P32;
+    if (fpr == MF_P32) {
+        k_to_f32<<<256, 256, 0, s>>>(x, x32, L);
+        MF_CUDA_TRY(cudaGetLastError());
+    }
+    SolverParams P;
+    fill_params(P, A, nullptr);
+    P.x = x;
+    P.p32 = x32;
+    int nsm = 0;
+    MF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const void *kfn = fpr == MF_P64 ? (const void *)k_spmv<MODE_FP64, 2> : (const void *)k_spmv<MODE_MIXED, 2>;
+    int occ = 1;
+    MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kThreads, 0));
+    if (occ < 1) occ = 1;
+    const int nhw_max = nsm * occ * kWarps * 2;
+    int rows_per_hw = (A->tilem + nhw_max - 1) / nhw_max;
+    if (rows_per_hw < 1) rows_per_hw = 1;
+    const int nhw = (A->tilem + rows_per_hw - 1) / rows_per_hw;
+    int blocks = (nhw + kWarps * 2 - 1) / (kWarps * 2);
+    if (blocks < 1) blocks = 1;
+    if (fpr == MF_P64) k_spmv<MODE_FP64, 2><<<blocks, kThreads, 0, s>>>(P, MF_P64, d_y, rows_per_hw);
+    else k_spmv<MODE_MIXED, 2><<<blocks, kThreads, 0, s>>>(P, MF_P32, d_y, rows_per_hw);
+    MF_CUDA_TRY(cudaGetLastError());
     return MF_SUCCESS;
 }

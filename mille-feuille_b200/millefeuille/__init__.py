@@ -162,6 +162,17 @@ class Matrix:
         self.last_spmv_ms = ms.value
         return y
 
+    def spmv_noalloc(self, x, y, precision="fp64", stream=None):
+        """y = A x through mf_spmv_noalloc: CUDA tensors only, asynchronous on
+        `stream`, no allocation inside the call (fixed scratch in the library)."""
+        L = _lib.load()
+        if not (_is_cuda_tensor(x) and _is_cuda_tensor(y)):
+            raise TypeError("spmv_noalloc takes CUDA tensors for x and y")
+        check(L.mf_spmv_noalloc(self._h, _ptr(x), _ptr(y),
+                                _PREC[precision] if isinstance(precision, str) else precision,
+                                C.c_void_p(stream) if stream else None), "mf_spmv_noalloc")
+        return y
+
 
 def read_matrix(path: str):
     """Reads .mtx / .cbd with the reference's semantics; returns
