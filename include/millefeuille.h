@@ -230,6 +230,24 @@ int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_p
 #define MF_SPMV_NOALLOC_MAX_LEN (1 << 21)
 int mf_spmv_noalloc(mf_matrix A, const double *x, double *y, int precision, void *stream);
 
+/* ------------------------------------------------- differentiation support
+ * No counterpart in the reference (it has no differentiation).  For
+ * A x = b and a loss L(x): lambda = A^-T dL/dx (an adjoint solve: the same
+ * solver on A for symmetric A, on a transposed handle otherwise), then
+ * dL/db = lambda and dL/dA = -lambda x^T on A's stored pattern.
+ */
+
+/* grad_val[e] = -sum_k lambda[k*n_rows + i] * x[k*n_cols + j] for every stored
+ * entry e = (i, j) of A, in the order of the CSR A was created from (entries of
+ * rows [0, n_rows)); nrhs right-hand sides stored one after another.  Pointers
+ * are host pointers unless device_ptrs != 0.  Deterministic. */
+int mf_value_grad(mf_matrix A, int nrhs, const double *lambda, const double *x, double *grad_val,
+                  int device_ptrs, void *stream);
+
+/* A handle for A^T (n_cols x n_rows), built from A's CSR; rows of A^T keep
+ * A's row order (stable, deterministic).  Destroy it with mf_matrix_destroy. */
+int mf_matrix_create_transposed(mf_matrix *out, mf_matrix A, void *stream);
+
 /* Test hook: segment labels of the reference rule for (p_old, p_new) device or
  * host arrays of length nseg*16; codes as d_vis (0 FP64, 4 FP32, 3 FP16, 2 INT8,
  * 1 bypass).  Runs the same device classifier the parity-mode solver uses. */

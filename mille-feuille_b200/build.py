@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
            "-ccbin", "g++", "-I", INCLUDE]
-SOURCES = ["scan.cu", "tile_build.cu", "solver.cu", "api.cu", "mmio.cpp"]
+SOURCES = ["scan.cu", "tile_build.cu", "solver.cu", "api.cu", "adjoint.cu", "mmio.cpp"]
 HEADERS = ["mf_internal.cuh"]
 
 

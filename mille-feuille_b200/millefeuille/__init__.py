@@ -162,6 +162,37 @@ class Matrix:
         self.last_spmv_ms = ms.value
         return y
 
+    def transposed(self, stream=None) -> "Matrix":
+        """A handle for A^T (mf_matrix_create_transposed)."""
+        L = _lib.load()
+        h = C.c_void_p()
+        check(L.mf_matrix_create_transposed(C.byref(h), self._h, C.c_void_p(stream) if stream else None),
+              "mf_matrix_create_transposed")
+        return Matrix(h)
+
+    def value_grad(self, lam, x, out=None, stream=None):
+        """dL/dA on the stored pattern: out[e] = -sum_k lam[k, i] x[k, j] for each
+        stored entry e = (i, j) (mf_value_grad).  lam: (n_rows,) or (nrhs, n_rows),
+        x: (n_cols,) or (nrhs, n_cols); numpy arrays or CUDA tensors (not mixed)."""
+        L = _lib.load()
+        dev = _is_cuda_tensor(lam)
+        nrhs = 1 if lam.ndim == 1 else int(lam.shape[0])
+        nnz = int(self.info["nnz"])
+        if dev:
+            import torch
+            lam = lam.contiguous()
+            x = x.contiguous()
+            if out is None:
+                out = torch.empty(nnz, dtype=torch.float64, device=lam.device)
+        else:
+            lam = np.ascontiguousarray(lam, dtype=np.float64)
+            x = np.ascontiguousarray(x, dtype=np.float64)
+            if out is None:
+                out = np.empty(nnz, dtype=np.float64)
+        check(L.mf_value_grad(self._h, nrhs, _ptr(lam), _ptr(x), _ptr(out), int(dev),
+                              C.c_void_p(stream) if stream else None), "mf_value_grad")
+        return out
+
     def spmv_noalloc(self, x, y, precision="fp64", stream=None):
         """y = A x through mf_spmv_noalloc: CUDA tensors only, asynchronous on
         `stream`, no allocation inside the call (fixed scratch in the library)."""

@@ -64,7 +64,7 @@ EXPORTED = [
     "mf_status_string", "cg_solve_inc", "cg_solve_sync", "cg_solve_reduce", "bicgstab", "bicgstab_sync",
     "bicgstab_inc", "mf_read_matrix", "mf_write_cbd", "mf_free_host", "mf_options_default", "mf_matrix_create",
     "mf_matrix_destroy", "mf_matrix_get_info", "mf_tile_array_bytes", "mf_tile_export", "mf_solve", "mf_spmv",
-    "mf_debug_ref_labels", "mf_build_arch", "mf_spmv_noalloc",
+    "mf_debug_ref_labels", "mf_build_arch", "mf_spmv_noalloc", "mf_value_grad", "mf_matrix_create_transposed",
 ]
 
 _lib = None
@@ -90,6 +90,8 @@ def load() -> C.CDLL:
     L.mf_solve.argtypes = [vp, vp, vp, C.POINTER(Options), C.POINTER(Report), C.c_int, vp]
     L.mf_spmv.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, dp]
     L.mf_spmv_noalloc.argtypes = [vp, vp, vp, C.c_int, vp]
+    L.mf_value_grad.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, vp]
+    L.mf_matrix_create_transposed.argtypes = [C.POINTER(vp), vp, vp]
     L.mf_debug_ref_labels.argtypes = [vp, vp, C.c_int, vp, C.c_int]
     L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
     L.mf_write_cbd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp]

@@ -157,6 +157,50 @@ def convdiff3d(N: int = 96, seed: int = 2, vscale: float = 10.0):
     return A, b, peclet
 
 
+def grf2d(N: int, corr: float, rng) -> np.ndarray:
+    """Gaussian random field on a periodic N x N grid: white noise (one
+    rng.standard_normal((N, N)) draw) convolved with exp(-r^2 / (2 corr^2)) by
+    FFT, scaled to zero mean and unit variance."""
+    w = rng.standard_normal((N, N))
+    d = np.minimum(np.arange(N), N - np.arange(N)).astype(np.float64)
+    ker = np.exp(-(d[:, None] ** 2 + d[None, :] ** 2) / (2.0 * corr * corr))
+    g = np.real(np.fft.ifft2(np.fft.fft2(w) * np.fft.fft2(ker)))
+    g -= g.mean()
+    return g / g.std()
+
+
+def aniso2d_grf(N: int = 512, seed: int = 4, corr: float = 16.0, ratio: float = 10.0, nrhs: int = 32):
+    """2D anisotropic diffusion on N x N cells (the differentiable-solve workload).
+
+    kappa = exp(GRF) with correlation length `corr` cells (grf2d, first draw of
+    default_rng(seed)); face coefficients are harmonic means of the two cells'
+    kappa, times `ratio` on x-faces (kappa_x = ratio kappa_y).  Dirichlet
+    boundary faces use the boundary cell's kappa (times ratio on x).
+    A = sum_f k_f (e_i - e_j)(e_i - e_j)^T + sum_boundary k_f e_i e_i^T (SPD).
+    Then B ~ N(0,1) (nrhs, n) and X_target ~ N(0,1) (nrhs, n), in that order.
+    Returns (A, B, X_target, kappa)."""
+    rng = np.random.default_rng(seed)
+    kap = np.exp(grf2d(N, corr, rng))          # kap[y, x]
+    kx = np.empty((N, N + 1))
+    ky = np.empty((N + 1, N))
+    kx[:, 1:N] = ratio * 2.0 * kap[:, :-1] * kap[:, 1:] / (kap[:, :-1] + kap[:, 1:])
+    ky[1:N, :] = 2.0 * kap[:-1, :] * kap[1:, :] / (kap[:-1, :] + kap[1:, :])
+    kx[:, 0], kx[:, N] = ratio * kap[:, 0], ratio * kap[:, N - 1]
+    ky[0, :], ky[N, :] = kap[0, :], kap[N - 1, :]
+    n = N * N
+    diag = (kx[:, :N] + kx[:, 1:] + ky[:N, :] + ky[1:, :]).reshape(n)
+    idx = np.arange(n, dtype=np.int64)
+    x, y = idx % N, idx // N
+    cols = np.stack([idx - N, idx - 1, idx, idx + 1, idx + N], axis=1)
+    mask = np.stack([y > 0, x > 0, np.ones(n, bool), x < N - 1, y < N - 1], axis=1)
+    vals = np.stack([-ky[:N, :].reshape(n), -kx[:, :N].reshape(n), diag, -kx[:, 1:].reshape(n),
+                     -ky[1:, :].reshape(n)], axis=1)
+    A = _from_slots(n, cols, vals, mask)
+    B = rng.standard_normal((nrhs, n))
+    Xt = rng.standard_normal((nrhs, n))
+    return A, B, Xt, kap
+
+
 def random_csr(n: int, ncols: int, density: float, seed: int, shuffle_cols: bool = True,
                empty_rows: float = 0.0, dense_tile_rows: int = 0) -> CSR:
     """Random CSR with unsorted columns (when shuffle_cols), optional empty rows

@@ -160,3 +160,24 @@ def test_generators_shapes():
     assert np.all(d >= off * (1 - 1e-14)) and np.any(d > off)   # weakly dominant, strictly on the boundary
     A, b, pe = M.convdiff3d(16, seed=2)
     assert A.n == 4096 and pe == pytest.approx(10 * (2 * np.pi / 16) / 2, rel=0.03)  # max sin at cell centres < 1
+
+
+def test_aniso2d_grf_generator():
+    """The differentiable-solve workload: SPD 5-point system, GRF of unit
+    variance, x-couplings ratio times the y-couplings, seeded."""
+    from millefeuille import matrices as M
+    A, B, Xt, kap = M.aniso2d_grf(64, seed=4, corr=16.0, nrhs=3)
+    assert A.n == 4096 and A.nnz == 5 * 4096 - 4 * 64 and B.shape == (3, 4096) and Xt.shape == (3, 4096)
+    g = np.log(kap)
+    assert abs(g.mean()) < 1e-12 and g.std() == pytest.approx(1.0, rel=1e-12)
+    S = A.to_scipy()
+    assert abs(S - S.T).max() == 0
+    d = S.diagonal()
+    off = np.asarray(abs(S).sum(axis=1)).ravel() - d
+    assert np.all(d >= off * (1 - 1e-14)) and np.any(d > off)
+    # interior cell 65 (x=1, y=1): x-coupling = 10 * harmonic mean of kappa, y-coupling = harmonic mean
+    hm = lambda a, b: 2 * a * b / (a + b)
+    assert S[65, 66] == pytest.approx(-10 * hm(kap[1, 1], kap[1, 2]), rel=1e-14)
+    assert S[65, 129] == pytest.approx(-hm(kap[1, 1], kap[2, 1]), rel=1e-14)
+    A2, B2, _, _ = M.aniso2d_grf(64, seed=4, corr=16.0, nrhs=3)
+    assert np.array_equal(A2.val, A.val) and np.array_equal(B2, B)
