@@ -10,7 +10,10 @@ iterations.  The input lives in HBM before the timed region; the matrix slice
 payload (hundreds of MB) is larger than the 126 MB L2, so no flush is needed
 between steps.  The same solve in all-FP64, the standalone FP64 tile SpMV (HBM
 GB/s, L2 flushed between launches) and an end-to-end solve through the public
-API with host buffers are reported beside it.
+API with host buffers are reported beside it, and so is the differentiable
+solve: forward + adjoint (backward) ms for 32 right-hand sides of the 512^2
+anisotropic GRF diffusion system through the autograd wrapper
+(config.fwd_adjoint).
 
 With N GPUs (torchrun) every rank solves its own replica (a single system does
 not shard; replicas only) and value = max-over-ranks time / (N * K).
@@ -239,10 +242,55 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": alg},
         "clocks": clk.summary(),
     }
+    if not args.no_adjoint:
+        out["config"]["fwd_adjoint"] = fwd_adjoint(dev, args.adjoint_rhs)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(A, b, rep64["iterations"], budget_s=args.cpu_budget)
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def fwd_adjoint(dev, nrhs):
+    """Differentiable CG on the 2D anisotropic GRF system (512^2 cells, kappa =
+    exp(GRF), correlation 16 cells, ratio 10, seed 4): loss = ||X - X_target||^2
+    over nrhs right-hand sides, forward solves then backward (adjoint solves +
+    value-gradient kernel), mixed precision, tol 1e-8 (about 10,500 CG
+    iterations per solve: no preconditioner, as in the reference), through the
+    autograd wrapper.  One untimed pass, then one timed pass (CUDA events)."""
+    import torch
+    from millefeuille import matrices as M
+    from millefeuille.autograd import SolvePattern, sparse_solve
+    A, B, Xt, _ = M.aniso2d_grf(512, seed=4, nrhs=nrhs)
+    rp = torch.from_numpy(A.rowptr).to(dev)
+    ci = torch.from_numpy(A.colidx).to(dev)
+    Bt = torch.from_numpy(B).to(dev)
+    Xtt = torch.from_numpy(Xt).to(dev)
+    pat = SolvePattern(rp, ci, A.n, symmetric=True)
+    res = {}
+    for timed in (False, True):
+        val = torch.from_numpy(A.val).to(dev).requires_grad_(True)
+        bt = Bt.clone().requires_grad_(True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize(dev)
+        e0.record()
+        x = sparse_solve(rp, ci, val, bt, method="cg", precision="mixed", tol=TOL, pattern=pat, max_iter=50000)
+        e1.record()
+        fwd_reps = list(pat.reports)
+        ((x - Xtt) ** 2).sum().backward()
+        e2.record()
+        torch.cuda.synchronize(dev)
+        if timed:
+            adj_reps = pat.reports
+            fwd_ms, tot_ms = e0.elapsed_time(e1), e0.elapsed_time(e2)
+            res = {"workload": f"aniso2d_grf_512 (n={A.n}, nnz={A.nnz}) x {nrhs} rhs, mixed CG tol 1e-8, "
+                               "loss ||X - X_target||^2, grads for b and A's values",
+                   "forward_ms": round(fwd_ms, 3), "fwd_adjoint_ms": round(tot_ms, 3),
+                   "ratio_fwd_adjoint_to_forward": round(tot_ms / fwd_ms, 3),
+                   "iterations_forward_mean": round(sum(r["iterations"] for r in fwd_reps) / len(fwd_reps), 1),
+                   "iterations_adjoint_mean": round(sum(r["iterations"] for r in adj_reps) / len(adj_reps), 1),
+                   "relres_true_max": max(r["relres_true"] for r in fwd_reps + adj_reps),
+                   "grad_val_norm": float(val.grad.norm()), "grad_b_norm": float(bt.grad.norm())}
+    return res
 
 
 def cpu_baseline(A, b, iters_to_tol, budget_s=12.0):
@@ -348,6 +396,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-solve (fwd+adjoint) line")
+    ap.add_argument("--adjoint-rhs", type=int, default=32)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     args = ap.parse_args()
     if args.profile:

@@ -195,6 +195,19 @@ int mf_tile_export(mf_matrix A, const char *name, void *host_dst, size_t bytes);
 int mf_solve(mf_matrix A, const double *b, double *x, const mf_options *opt, mf_report *report,
              int device_ptrs, void *stream);
 
+/*
+ * Solve A X = B for nrhs right-hand sides (CG; MF_PREC_FP64 or MF_PREC_MIXED).
+ * B and X hold nrhs vectors of n_rows doubles one after another; host
+ * pointers unless device_ptrs != 0.  Up to 8 columns run in one persistent
+ * launch (every matrix entry read once per SpMV for all of them, one grid sync
+ * for all of them); each column has its own alpha / beta, convergence test
+ * and FP64 true-residual check.  reports (nullable) receives nrhs records
+ * (time_ms and replacements are those of the column's launch).  nrhs == 1 is
+ * mf_solve.  No counterpart in the reference (one right-hand side per call).
+ */
+int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_options *opt,
+                   mf_report *reports, int device_ptrs, void *stream);
+
 /* y = A x with the tile kernel.  precision: MF_PREC_FP64 or MF_PREC_MIXED
  * (MIXED here means every tile in FP32).  elapsed_ms (nullable) gets the kernel time. */
 int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs,

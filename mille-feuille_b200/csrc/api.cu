@@ -303,6 +303,37 @@ extern "C" int mf_solve(mf_matrix A, const double *b, double *x, const mf_option
     return rc;
 }
 
+extern "C" int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_options *opt,
+                              mf_report *reports, int device_ptrs, void *stream)
+{
+    if (!A || !B || !X || nrhs < 1) return MF_ERR_INVALID;
+    if (A->n_rows != A->n_cols) return MF_ERR_INVALID;
+    mf_options o;
+    if (opt) o = *opt;
+    else mf_options_default(&o);
+    if (nrhs == 1) {
+        // one column: the single-column kernel
+        return mf_solve(A, B, X, &o, reports, device_ptrs, stream);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = (size_t)nrhs * A->n_rows * sizeof(double);
+    const double *dB = B;
+    double *dX = X, *tmp = nullptr;
+    if (!device_ptrs) {
+        MF_CUDA_TRY(cudaMallocAsync((void **)&tmp, 2 * bytes, s));
+        MF_CUDA_TRY(cudaMemcpyAsync(tmp, B, bytes, cudaMemcpyHostToDevice, s));
+        dB = tmp;
+        dX = tmp + (size_t)nrhs * A->n_rows;
+    }
+    int rc = mf_solver_multi_run(A, nrhs, dB, dX, &o, reports, s);
+    if (!device_ptrs) {
+        cudaMemcpyAsync(X, dX, bytes, cudaMemcpyDeviceToHost, s);
+        cudaFreeAsync(tmp, s);
+        MF_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return rc;
+}
+
 extern "C" int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs, void *stream,
                        double *elapsed_ms)
 {

@@ -113,6 +113,8 @@ int mf_build_tiles(mf_matrix_s *A, cudaStream_t s);
 // solver (solver.cu)
 int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_options *opt,
                   mf_report *rep, cudaStream_t s);
+int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X, const mf_options *opt,
+                        mf_report *reps, cudaStream_t s);
 int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s,
                 double *elapsed_ms);
 int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s);

@@ -79,7 +79,8 @@ struct Shared {
 };
 
 // ------------------------------------------------------------ grid barrier
-__device__ bool grid_barrier(const SolverParams &P, unsigned &epoch, Shared &sh)
+template <class SH>
+__device__ bool grid_barrier(const SolverParams &P, unsigned &epoch, SH &sh)
 {
     __syncthreads();
     epoch += 1;
@@ -1088,6 +1089,486 @@ __global__ void k_ref_labels(const double *pold, const double *pnew, int nseg, i
     if (valid && i == 0) vis[seg] = rank_to_vis(m);
 }
 
+// ------------------------------------------------------------ several right-hand sides
+// CG on NR right-hand sides at once (FP64 and mixed modes): the vectors are
+// interleaved (row i's NR values contiguous), so every matrix entry is read
+// once per SpMV for all NR columns and one grid sync serves every column; the
+// scalars alpha_k, beta_k and the convergence state are per column.  Same
+// two-sync schedule as the single-column kernel (SpMV on R; P = R + beta P,
+// Q = W + beta Q; then X += alpha P, R -= alpha Q).
+constexpr int kMaxNR = 8;
+constexpr int kRedWidthM = kMaxNR + 2;    // NR dot products + segment max / -min
+
+struct SharedM {
+    double wred[kWarps][kRedWidthM];
+    double bcast[kRedWidthM];
+    double alpha[kMaxNR], beta[kMaxNR], rr[kMaxNR], thr2[kMaxNR], bb[kMaxNR];
+    int active[kMaxNR], pending[kMaxNR], iters[kMaxNR], conv[kMaxNR];
+    int brk;                  // some column broke down (a scalar became non-finite)
+    int flag;                 // grid_barrier's result
+};
+
+struct MultiParams {
+    const double *B;          // [vec_len * NR] interleaved right-hand sides (zero columns past nr)
+    double *X, *R, *Pv, *Q;   // interleaved
+    float *R32;               // interleaved FP32 shadow of R (mixed)
+    float *mag;               // per tile-row: max over its rows and columns of |R|
+    double *red;              // [kinds][G][kRedWidthM]
+    double *out;              // per column: iterations, converged, true rel. residual, recursive; then k, status
+    int nr;                   // columns in use
+};
+
+// Block partial of NV values (maxmask bit k: max instead of sum) into red[kind][block][*].
+template <int NV>
+__device__ void block_partial_m(const MultiParams &M, SharedM &sh, int kind, const double (&v)[NV], unsigned maxmask)
+{
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        double a = v[k];
+        const bool mx = (maxmask >> k) & 1u;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double b = __shfl_xor_sync(0xffffffffu, a, o);
+            a = mx ? fmax(a, b) : a + b;
+        }
+        if (lane == 0) sh.wred[wib][k] = a;
+    }
+    __syncthreads();
+    // warp w reduces value w (fixed order)
+    if (wib < NV) {
+        const bool mx = (maxmask >> wib) & 1u;
+        double a = (lane < kWarps) ? sh.wred[lane][wib] : (mx ? -1.0e300 : 0.0);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double b = __shfl_xor_sync(0xffffffffu, a, o);
+            a = mx ? fmax(a, b) : a + b;
+        }
+        if (lane == 0) M.red[((long long)kind * gridDim.x + blockIdx.x) * kRedWidthM + wib] = a;
+    }
+}
+
+// After the sync: every block sums the block partials of `kind` in the same order.
+template <int NV>
+__device__ void grid_collect_m(const MultiParams &M, SharedM &sh, int kind, unsigned maxmask, double (&out)[NV])
+{
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    if (wib < NV) {
+        const bool mx = (maxmask >> wib) & 1u;
+        double a = mx ? -1.0e300 : 0.0;
+        for (int c = lane; c < (int)gridDim.x; c += 32) {
+            const double b = M.red[((long long)kind * gridDim.x + c) * kRedWidthM + wib];
+            a = mx ? fmax(a, b) : a + b;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double b = __shfl_xor_sync(0xffffffffu, a, o);
+            a = mx ? fmax(a, b) : a + b;
+        }
+        if (lane == 0) sh.bcast[wib] = a;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; k++) out[k] = sh.bcast[k];
+    __syncthreads();
+}
+
+// Y = A X for NR interleaved columns over the half-warp's slices; epi(R, acc)
+// once per tile-row with lane i's NR row sums.  Precision per slice as in
+// slice_dot (mixed: from the column segments' max over rows and columns).
+template <int MODE, int NR, bool F64, typename Epi>
+__device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se, int i, unsigned hmask,
+                                           const double *X64, const float *X32, const float *mag, float invM,
+                                           Epi epi)
+{
+    constexpr bool kMixed = (MODE == MODE_MIXED) && !F64;
+    XVec X = make_x(X64, X32, nullptr, nullptr, mag, nullptr, invM);
+    double acc[NR];
+#pragma unroll
+    for (int k = 0; k < NR; k++) acc[k] = 0.0;
+    if (sb >= se) return;
+    int4 h = P.seg_hdr[sb];
+    int tw = P.seg_tile[(long long)sb * MF_BS + i];
+    int len = P.seg_rowlen[(long long)sb * MF_BS + i];
+    for (int s = sb; s < se; s++) {
+        const bool more = s + 1 < se;
+        int4 hn = make_int4(0, 0, 0, 0);
+        int twn = 0, lenn = 0;
+        if (more) {
+            hn = P.seg_hdr[s + 1];
+            twn = P.seg_tile[(long long)(s + 1) * MF_BS + i];
+            lenn = P.seg_rowlen[(long long)(s + 1) * MF_BS + i];
+        }
+        const int xb = (tw >> 8) * MF_BS;
+        int pr = MF_P64;
+        if (kMixed) {
+            const float st = (i < hdr_nt(h)) ? mag[tw >> 8] : 0.0f;
+            pr = (i < hdr_nt(h)) ? tile_prec<MODE, false>(P, tw, st, X) : MF_P8;
+#pragma unroll
+            for (int o = 8; o; o >>= 1) pr = min(pr, __shfl_xor_sync(hmask, pr, o));
+        }
+        float sc = 0.0f;
+        if (kMixed && pr == MF_P8) sc = (i < hdr_nt(h)) ? P.i8_scale[h.x + i] : 0.0f;
+        const int kp = hdr_kp(h);
+        const long long off = hdr_off(h);
+        const unsigned long long *mrow = (const unsigned long long *)(P.meta + off + (long long)i * kp);
+        for (int k0 = 0; k0 < kp; k0 += 8) {
+            const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
+            if (!kMixed || pr == MF_P64) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+                    const int xi = __shfl_sync(hmask, xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
+                    if (k0 + j < len) {
+                        const double v = __ldcs(P.v64 + off + (long long)(k0 + j) * MF_BS + i);
+                        const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
+#pragma unroll
+                        for (int q = 0; q < NR / 2; q++) {
+                            const double2 d = xr[q];
+                            acc[2 * q] = fma(v, d.x, acc[2 * q]);
+                            acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
+                        }
+                    }
+                }
+            } else {
+                float part[NR];
+#pragma unroll
+                for (int k = 0; k < NR; k++) part[k] = 0.0f;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+                    const int slot = (int)(mm >> 4);
+                    const int xi = __shfl_sync(hmask, xb, slot, 16) + (int)(mm & 15u);
+                    const float s8 = (pr == MF_P8) ? __shfl_sync(hmask, sc, slot, 16) : 0.0f;
+                    if (k0 + j < len) {
+                        const long long e = off + (long long)(k0 + j) * MF_BS + i;
+                        const float v = (pr == MF_P32)   ? __ldcs(P.v32 + e)
+                                        : (pr == MF_P16) ? __half2float(P.v16[e])
+                                                         : (float)P.v8[e] * s8;
+                        const float2 *xr = (const float2 *)(X32 + (long long)xi * NR);
+#pragma unroll
+                        for (int q = 0; q < NR / 2; q++) {
+                            const float2 d = xr[q];
+                            part[2 * q] = fmaf(v, d.x, part[2 * q]);
+                            part[2 * q + 1] = fmaf(v, d.y, part[2 * q + 1]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < NR; k++) acc[k] += (double)part[k];
+            }
+        }
+        if (hdr_last(h)) {
+            epi(h.y, acc);
+#pragma unroll
+            for (int k = 0; k < NR; k++) acc[k] = 0.0;
+        }
+        h = hn;
+        tw = twn;
+        len = lenn;
+    }
+}
+
+// Largest / smallest segment magnitude of the SpMV operand (mixed mode).
+struct SegMM {
+    float mx, mn;
+};
+
+// R's FP32 shadow and segment magnitude (max over the tile-row's rows and all
+// columns) for tile-row R; all 16 lanes of the half-warp call it together.
+template <int MODE, int NR>
+__device__ __forceinline__ void publish_multi(const MultiParams &M, int R, int row, bool valid, const double (&rv)[NR],
+                                              SegMM &st, unsigned hmask)
+{
+    if (MODE != MODE_MIXED) return;
+    float m = 0.0f;
+    if (valid) {
+        float2 *dst = (float2 *)(M.R32 + (long long)row * NR);
+#pragma unroll
+        for (int q = 0; q < NR / 2; q++) {
+            dst[q] = make_float2((float)rv[2 * q], (float)rv[2 * q + 1]);
+            m = fmaxf(m, fmaxf(fabsf((float)rv[2 * q]), fabsf((float)rv[2 * q + 1])));
+        }
+    }
+    m = half_max(m, hmask);
+    st.mx = fmaxf(st.mx, m);
+    st.mn = fminf(st.mn, m);
+    if ((threadIdx.x & 15) == 0) M.mag[R] = m;
+}
+
+template <int NR>
+__device__ __forceinline__ void load_row(const double *v, int row, double (&out)[NR])
+{
+    const double2 *p = (const double2 *)(v + (long long)row * NR);
+#pragma unroll
+    for (int q = 0; q < NR / 2; q++) {
+        const double2 d = p[q];
+        out[2 * q] = d.x;
+        out[2 * q + 1] = d.y;
+    }
+}
+template <int NR>
+__device__ __forceinline__ void store_row(double *v, int row, const double (&in)[NR])
+{
+    double2 *p = (double2 *)(v + (long long)row * NR);
+#pragma unroll
+    for (int q = 0; q < NR / 2; q++) p[q] = make_double2(in[2 * q], in[2 * q + 1]);
+}
+
+template <int MODE, int NR>
+__global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, MultiParams M)
+{
+    __shared__ SharedM sh;
+    const Ctx c = make_ctx(P);
+    unsigned epoch = 0;
+    const int n = P.n;
+    bool has_empty = false;
+    for (int R = c.rbeg; R < c.rend && !has_empty; R++) has_empty = P.seg_ptr[R] == P.seg_ptr[R + 1];
+    const unsigned mm2 = 3u << NR;          // the two trailing max slots
+
+    // ---- init: X = 0, R = B, P = Q = 0; |b_k|^2; R's shadow ----
+    double pb[NR + 2];
+#pragma unroll
+    for (int k = 0; k < NR + 2; k++) pb[k] = 0.0;
+    SegMM st = {0.0f, 3.0e38f};
+    for (int R = c.rbeg; R < c.rend; R++) {
+        const int row = R * MF_BS + c.i;
+        const bool valid = row < n;
+        double rv[NR], z[NR];
+#pragma unroll
+        for (int k = 0; k < NR; k++) { rv[k] = 0.0; z[k] = 0.0; }
+        if (valid) {
+            load_row<NR>(M.B, row, rv);
+            store_row<NR>(M.X, row, z);
+            store_row<NR>(M.R, row, rv);
+            store_row<NR>(M.Pv, row, z);
+            store_row<NR>(M.Q, row, z);
+#pragma unroll
+            for (int k = 0; k < NR; k++) pb[k] += rv[k] * rv[k];
+        }
+        publish_multi<MODE, NR>(M, R, row, valid, rv, st, c.hmask);
+    }
+    pb[NR] = st.mx;
+    pb[NR + 1] = -st.mn;
+    block_partial_m<NR + 2>(M, sh, 0, pb, mm2);
+    if (!grid_barrier(P, epoch, sh)) return;
+    double v[NR + 2];
+    grid_collect_m<NR + 2>(M, sh, 0, mm2, v);
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < NR; k++) {
+            sh.bb[k] = v[k];
+            sh.rr[k] = v[k];
+            sh.thr2[k] = P.tol * P.tol * v[k];
+            sh.beta[k] = 0.0;
+            sh.pending[k] = 0;
+            sh.iters[k] = 0;
+            sh.conv[k] = (k < M.nr && !P.fixed_iters && v[k] <= sh.thr2[k]) ? 1 : 0;
+            sh.active[k] = (k < M.nr && !sh.conv[k]) ? 1 : 0;
+        }
+        sh.brk = 0;
+    }
+    __syncthreads();
+    float invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
+    int k = 0, status = 0, repl = 0, last_true = 0;
+    double rt[NR];
+#pragma unroll
+    for (int j = 0; j < NR; j++) rt[j] = v[j];
+
+    for (;;) {
+        int any = 0;
+#pragma unroll
+        for (int j = 0; j < NR; j++) any |= sh.active[j];
+        if (!any || k >= P.max_iter) break;
+        // ---- A: W = A R; P = R + beta P; Q = W + beta Q; P.Q per column ----
+        double ppq[NR];
+#pragma unroll
+        for (int j = 0; j < NR; j++) ppq[j] = 0.0;
+        auto upd_a = [&](int R, const double (&w)[NR]) {
+            const int row = R * MF_BS + c.i;
+            if (row < n) {
+                double r[NR], p[NR], q[NR];
+                load_row<NR>(M.R, row, r);
+                load_row<NR>(M.Pv, row, p);
+                load_row<NR>(M.Q, row, q);
+#pragma unroll
+                for (int j = 0; j < NR; j++) {
+                    p[j] = r[j] + sh.beta[j] * p[j];
+                    q[j] = w[j] + sh.beta[j] * q[j];
+                    ppq[j] += p[j] * q[j];
+                }
+                store_row<NR>(M.Pv, row, p);
+                store_row<NR>(M.Q, row, q);
+            }
+        };
+        spmv_multi<MODE, NR, false>(P, c.sbeg, c.send, c.i, c.hmask, M.R, M.R32, M.mag, invM, upd_a);
+        if (has_empty) {
+            double zw[NR];
+#pragma unroll
+            for (int j = 0; j < NR; j++) zw[j] = 0.0;
+            for (int R = c.rbeg; R < c.rend; R++)
+                if (P.seg_ptr[R] == P.seg_ptr[R + 1]) upd_a(R, zw);
+        }
+        block_partial_m<NR>(M, sh, 1, ppq, 0u);
+        if (!grid_barrier(P, epoch, sh)) return;
+        double pq[NR];
+        grid_collect_m<NR>(M, sh, 1, 0u, pq);
+        if (threadIdx.x == 0) {
+            for (int j = 0; j < NR; j++) {
+                double a = sh.active[j] ? sh.rr[j] / pq[j] : 0.0;
+                if (!isfinite(a)) {      // breakdown of this column: it stops where it is
+                    a = 0.0;
+                    sh.active[j] = 0;
+                    sh.brk = 1;
+                }
+                sh.alpha[j] = a;
+            }
+        }
+        __syncthreads();
+        if (sh.brk) status = MF_ERR_BREAKDOWN;
+        // ---- B: X += alpha P; R -= alpha Q; R.R; R's shadow ----
+        double prr[NR + 2];
+#pragma unroll
+        for (int j = 0; j < NR + 2; j++) prr[j] = 0.0;
+        st = SegMM{0.0f, 3.0e38f};
+        for (int R = c.rbeg; R < c.rend; R++) {
+            const int row = R * MF_BS + c.i;
+            const bool valid = row < n;
+            double r[NR];
+#pragma unroll
+            for (int j = 0; j < NR; j++) r[j] = 0.0;
+            if (valid) {
+                double x[NR], p[NR], q[NR];
+                load_row<NR>(M.X, row, x);
+                load_row<NR>(M.Pv, row, p);
+                load_row<NR>(M.R, row, r);
+                load_row<NR>(M.Q, row, q);
+#pragma unroll
+                for (int j = 0; j < NR; j++) {
+                    x[j] += sh.alpha[j] * p[j];
+                    r[j] -= sh.alpha[j] * q[j];
+                    prr[j] += r[j] * r[j];
+                }
+                store_row<NR>(M.X, row, x);
+                store_row<NR>(M.R, row, r);
+            }
+            publish_multi<MODE, NR>(M, R, row, valid, r, st, c.hmask);
+        }
+        prr[NR] = st.mx;
+        prr[NR + 1] = -st.mn;
+        block_partial_m<NR + 2>(M, sh, 2, prr, mm2);
+        if (!grid_barrier(P, epoch, sh)) return;
+        grid_collect_m<NR + 2>(M, sh, 2, mm2, v);
+        invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
+        k++;
+        last_true = 0;
+        bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
+#pragma unroll
+        for (int j = 0; j < NR; j++)
+            if (sh.active[j] && !P.fixed_iters && v[j] <= sh.thr2[j]) want_repl = true;
+        double rnew[NR];
+#pragma unroll
+        for (int j = 0; j < NR; j++) rnew[j] = v[j];
+        if (want_repl) {
+            // ---- FP64 R = B - A X, R's shadow, true residual norms ----
+            double prt[NR + 2];
+#pragma unroll
+            for (int j = 0; j < NR + 2; j++) prt[j] = 0.0;
+            st = SegMM{0.0f, 3.0e38f};
+            auto upd_r = [&](int R, const double (&y)[NR]) {
+                const int row = R * MF_BS + c.i;
+                const bool valid = row < n;
+                double r[NR];
+#pragma unroll
+                for (int j = 0; j < NR; j++) r[j] = 0.0;
+                if (valid) {
+                    load_row<NR>(M.B, row, r);
+#pragma unroll
+                    for (int j = 0; j < NR; j++) {
+                        r[j] -= y[j];
+                        prt[j] += r[j] * r[j];
+                    }
+                    store_row<NR>(M.R, row, r);
+                }
+                publish_multi<MODE, NR>(M, R, row, valid, r, st, c.hmask);
+            };
+            spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, upd_r);
+            if (has_empty) {
+                double zy[NR];
+#pragma unroll
+                for (int j = 0; j < NR; j++) zy[j] = 0.0;
+                for (int R = c.rbeg; R < c.rend; R++)
+                    if (P.seg_ptr[R] == P.seg_ptr[R + 1]) upd_r(R, zy);
+            }
+            prt[NR] = st.mx;
+            prt[NR + 1] = -st.mn;
+            block_partial_m<NR + 2>(M, sh, 5, prt, mm2);
+            if (!grid_barrier(P, epoch, sh)) return;
+            grid_collect_m<NR + 2>(M, sh, 5, mm2, v);
+            invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
+            repl++;
+            last_true = 1;
+#pragma unroll
+            for (int j = 0; j < NR; j++) {
+                rt[j] = v[j];
+                rnew[j] = v[j];
+            }
+        }
+        if (threadIdx.x == 0) {
+            for (int j = 0; j < NR; j++) {
+                if (sh.active[j] && last_true && !P.fixed_iters && rnew[j] <= sh.thr2[j]) {
+                    sh.active[j] = 0;            // converged on the FP64 true residual
+                    sh.conv[j] = 1;
+                    sh.iters[j] = k;
+                }
+                sh.beta[j] = sh.active[j] ? rnew[j] / sh.rr[j] : 0.0;
+                if (sh.active[j] || !sh.conv[j]) sh.rr[j] = rnew[j];
+            }
+        }
+        __syncthreads();
+    }
+    // ---- final FP64 true residuals when the last step did not form them ----
+    if (!last_true) {
+        double prt[NR];
+#pragma unroll
+        for (int j = 0; j < NR; j++) prt[j] = 0.0;
+        auto acc_r = [&](int R, const double (&y)[NR]) {
+            const int row = R * MF_BS + c.i;
+            if (row < n) {
+                double b[NR];
+                load_row<NR>(M.B, row, b);
+#pragma unroll
+                for (int j = 0; j < NR; j++) prt[j] += (b[j] - y[j]) * (b[j] - y[j]);
+            }
+        };
+        spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, acc_r);
+        if (has_empty) {
+            double zy[NR];
+#pragma unroll
+            for (int j = 0; j < NR; j++) zy[j] = 0.0;
+            for (int R = c.rbeg; R < c.rend; R++)
+                if (P.seg_ptr[R] == P.seg_ptr[R + 1]) acc_r(R, zy);
+        }
+        block_partial_m<NR>(M, sh, 7, prt, 0u);
+        if (!grid_barrier(P, epoch, sh)) return;
+        double w[NR];
+        grid_collect_m<NR>(M, sh, 7, 0u, w);
+#pragma unroll
+        for (int j = 0; j < NR; j++) rt[j] = w[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int j = 0; j < NR; j++) {
+            const double bb = sh.bb[j];
+            M.out[4 * j + 0] = (double)(sh.conv[j] ? sh.iters[j] : k);
+            M.out[4 * j + 1] = (double)sh.conv[j];
+            M.out[4 * j + 2] = bb > 0 ? sqrt(rt[j] / bb) : 0.0;
+            M.out[4 * j + 3] = bb > 0 ? sqrt(sh.rr[j] / bb) : 0.0;
+        }
+        M.out[4 * NR + 0] = (double)k;
+        M.out[4 * NR + 1] = (double)status;
+        M.out[4 * NR + 2] = (double)repl;
+    }
+}
+
 // ------------------------------------------------------------ workspace
 struct Workspace {
     int G;                 // grid blocks of the persistent kernel
@@ -1110,6 +1591,12 @@ struct Workspace {
     int *hw_begin;
     int nhw;
     cudaEvent_t e0, e1;
+    // several right-hand sides (k_solve_multi): interleaved vectors for NR columns
+    int m_nr, m_G;
+    double *m_vec;         // B | X | R | P | Q, each vec_len * NR
+    float *m_r32, *m_mag;
+    double *m_red, *m_out;
+    int *m_hw_begin;
 };
 
 template <typename T>
@@ -1300,7 +1787,7 @@ void mf_solver_free_ws(mf_matrix_s *A)
     Workspace *w = (Workspace *)A->ws;
     if (!w) return;
     void *ptrs[] = {w->vecs, w->mag_p, w->mag_s, w->lab_p, w->lab_s, w->red, w->bar, w->err, w->out, w->counts,
-                    w->phase_ns, w->hw_begin};
+                    w->phase_ns, w->hw_begin, w->m_vec, w->m_r32, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     cudaEventDestroy(w->e0);
@@ -1533,4 +2020,155 @@ int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int prec
     else k_spmv<MODE_MIXED, 2><<<blocks, kThreads, 0, s>>>(P, MF_P32, d_y, rows_per_hw);
     MF_CUDA_TRY(cudaGetLastError());
     return MF_SUCCESS;
+}
+
+// ------------------------------------------------------------ several right-hand sides (host)
+namespace {
+
+// column block g of B (nrhs x n, one column after another) -> interleaved [row * NR + k]
+__global__ void k_interleave(const double *B, int n, int L, int nrhs, int g, int NR, double *Bi)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)L * NR;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int row = (int)(t / NR), k = (int)(t % NR), col = g * NR + k;
+        Bi[t] = (row < n && col < nrhs) ? B[(long long)col * n + row] : 0.0;
+    }
+}
+__global__ void k_deinterleave(const double *Xi, int n, int nrhs, int g, int NR, double *X)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)n * NR;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int row = (int)(t / NR), k = (int)(t % NR), col = g * NR + k;
+        if (col < nrhs) X[(long long)col * n + row] = Xi[t];
+    }
+}
+
+const void *multi_kernel(int mode, int nr)
+{
+    if (mode == MODE_FP64)
+        return nr == 2 ? (const void *)k_solve_multi<MODE_FP64, 2>
+               : nr == 4 ? (const void *)k_solve_multi<MODE_FP64, 4> : (const void *)k_solve_multi<MODE_FP64, 8>;
+    return nr == 2 ? (const void *)k_solve_multi<MODE_MIXED, 2>
+           : nr == 4 ? (const void *)k_solve_multi<MODE_MIXED, 4> : (const void *)k_solve_multi<MODE_MIXED, 8>;
+}
+
+// The multi-column workspace for NR columns (grid: one block of 512 threads per SM).
+int ws_multi(mf_matrix_s *A, Workspace *w, int mode, int nr, cudaStream_t s)
+{
+    if (w->m_nr == nr && w->m_vec) return MF_SUCCESS;
+    void *old[] = {w->m_vec, w->m_r32, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
+    for (void *p : old)
+        if (p) cudaFree(p);
+    w->m_vec = nullptr; w->m_r32 = nullptr; w->m_mag = nullptr; w->m_red = nullptr; w->m_out = nullptr;
+    w->m_hw_begin = nullptr;
+    w->m_nr = 0;
+    int dev = 0, nsm = 0, occ = 0;
+    MF_CUDA_TRY(cudaGetDevice(&dev));
+    MF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    for (int m = MODE_FP64; m <= MODE_MIXED; m++) {
+        int o = 0;
+        MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, multi_kernel(m, nr), kThreads, 0));
+        occ = (m == MODE_FP64 || o < occ) ? o : occ;
+    }
+    if (occ < 1) return MF_ERR_UNSUPPORTED;
+    int G = nsm * (occ > 1 ? 1 : occ);
+    const int need = (A->tilem + kWarps * 2 - 1) / (kWarps * 2);
+    if (need < G) G = need > 0 ? need : 1;
+    const long long L = A->vec_len, S = std::max(A->tilem, A->tilen) + 1;
+    MF_TRY(dal(&w->m_vec, 5 * L * nr));
+    MF_TRY(dal(&w->m_r32, L * nr));
+    MF_TRY(dal(&w->m_mag, S));
+    MF_TRY(dal(&w->m_red, (long long)kRedKinds * G * kRedWidthM));
+    MF_TRY(dal(&w->m_out, 4 * kMaxNR + 8));
+    MF_TRY(dal(&w->m_hw_begin, (long long)G * kWarps * 2 + 1));
+    MF_CUDA_TRY(cudaMemsetAsync(w->m_vec, 0, (size_t)5 * L * nr * sizeof(double), s));
+    MF_CUDA_TRY(cudaMemsetAsync(w->m_r32, 0, (size_t)L * nr * sizeof(float), s));
+    MF_CUDA_TRY(cudaMemsetAsync(w->m_mag, 0, (size_t)S * sizeof(float), s));
+    const int nhw = G * kWarps * 2;
+    k_partition<<<(nhw + 256) / 256, 256, 0, s>>>(A->d_row_cost, A->tilem, nhw, w->m_hw_begin);
+    MF_CUDA_TRY(cudaGetLastError());
+    w->m_G = G;
+    w->m_nr = nr;
+    return MF_SUCCESS;
+}
+
+}  // namespace
+
+int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X, const mf_options *opt,
+                        mf_report *reps, cudaStream_t s)
+{
+    if (opt->method != MF_METHOD_CG || opt->precision == MF_PREC_PARITY) return MF_ERR_UNSUPPORTED;
+    if (opt->x0_given) return MF_ERR_UNSUPPORTED;
+    const int mode = opt->precision == MF_PREC_FP64 ? MODE_FP64 : MODE_MIXED;
+    Workspace *w = nullptr;
+    MF_TRY(ws_get(A, opt->blocks_per_sm, &w, s));
+    const int nr = nrhs >= 8 ? 8 : nrhs >= 4 ? 4 : 2;   // columns per launch
+    MF_TRY(ws_multi(A, w, mode, nr, s));
+    const long long L = A->vec_len;
+    const int n = A->n_rows;
+    SolverParams P;
+    fill_params(P, A, w);
+    P.hw_begin = w->m_hw_begin;
+    P.method = MF_METHOD_CG;
+    P.max_iter = opt->max_iter;
+    P.fixed_iters = opt->fixed_iters;
+    P.replace_every = opt->replace_every;
+    P.use_lossless = opt->use_lossless;
+    P.tol = opt->tol;
+    P.demote16 = (float)opt->demote_fp16;
+    P.demote8 = (float)opt->demote_int8;
+    const double to = opt->wait_timeout_s > 0 ? opt->wait_timeout_s : 10.0;
+    P.timeout_ns = (unsigned long long)(to * 1e9);
+    P.stall_first_barrier = opt->test_stall_barrier ? 1 : 0;
+    MultiParams M;
+    M.B = w->m_vec;
+    M.X = w->m_vec + L * nr;
+    M.R = w->m_vec + 2 * L * nr;
+    M.Pv = w->m_vec + 3 * L * nr;
+    M.Q = w->m_vec + 4 * L * nr;
+    M.R32 = w->m_r32;
+    M.mag = w->m_mag;
+    M.red = w->m_red;
+    M.out = w->m_out;
+    const int groups = (nrhs + nr - 1) / nr;
+    int first_err = MF_SUCCESS;
+    for (int g = 0; g < groups; g++) {
+        M.nr = std::min(nr, nrhs - g * nr);
+        k_interleave<<<592, 256, 0, s>>>(d_B, n, (int)L, nrhs, g, nr, (double *)M.B);
+        MF_CUDA_TRY(cudaGetLastError());
+        MF_CUDA_TRY(cudaMemsetAsync(w->bar, 0, sizeof(unsigned int), s));
+        MF_CUDA_TRY(cudaMemsetAsync(w->err, 0, sizeof(int), s));
+        MF_CUDA_TRY(cudaMemsetAsync(w->m_out, 0, (4 * kMaxNR + 8) * sizeof(double), s));
+        void *args[] = {&P, &M};
+        MF_CUDA_TRY(cudaEventRecord(w->e0, s));
+        MF_CUDA_TRY(cudaLaunchCooperativeKernel(multi_kernel(mode, nr), dim3(w->m_G), dim3(kThreads), args, 0, s));
+        MF_CUDA_TRY(cudaEventRecord(w->e1, s));
+        k_deinterleave<<<592, 256, 0, s>>>(M.X, n, nrhs, g, nr, d_X);
+        MF_CUDA_TRY(cudaGetLastError());
+        double out[4 * kMaxNR + 8];
+        int err = 0;
+        MF_CUDA_TRY(cudaMemcpyAsync(out, w->m_out, sizeof(out), cudaMemcpyDeviceToHost, s));
+        MF_CUDA_TRY(cudaMemcpyAsync(&err, w->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MF_CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        MF_CUDA_TRY(cudaEventElapsedTime(&ms, w->e0, w->e1));
+        const int status = err ? err : (int)out[4 * nr + 1];
+        if (status != MF_SUCCESS && first_err == MF_SUCCESS) first_err = status;
+        if (reps) {
+            for (int k = 0; k < M.nr; k++) {
+                mf_report *r = &reps[g * nr + k];
+                memset(r, 0, sizeof(*r));
+                r->status = status;
+                r->iterations = (int)out[4 * k + 0];
+                r->converged = (int)out[4 * k + 1];
+                r->relres_true = out[4 * k + 2];
+                r->relres_rec = out[4 * k + 3];
+                r->time_ms = ms;
+                r->replacements = (int)out[4 * nr + 2];
+                r->grid_blocks = w->m_G;
+                r->threads_per_block = kThreads;
+            }
+        }
+    }
+    return first_err;
 }

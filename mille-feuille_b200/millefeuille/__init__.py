@@ -145,6 +145,36 @@ class Matrix:
             raise err
         return x, rep.as_dict()
 
+    def solve_multi(self, B, X=None, options: Options | None = None, stream=None, **kw):
+        """Solve A X = B for the rows of B (shape (nrhs, n)) with mf_solve_multi:
+        up to 8 right-hand sides per persistent launch.  Returns (X, list of
+        report dicts); raises MFError on failure (reports attached)."""
+        L = _lib.load()
+        o = options if options is not None else default_options(**kw)
+        if options is not None and kw:
+            for k, v in kw.items():
+                setattr(o, k, _PREC.get(v, v) if k == "precision" else _METHOD.get(v, v) if k == "method" else v)
+        dev = _is_cuda_tensor(B)
+        if dev:
+            import torch
+            B = B.contiguous()
+            if X is None:
+                X = torch.zeros_like(B)
+        else:
+            B = np.ascontiguousarray(B, dtype=np.float64)
+            if X is None:
+                X = np.zeros_like(B)
+        nrhs = int(B.shape[0])
+        reps = (Report * nrhs)()
+        st = L.mf_solve_multi(self._h, nrhs, _ptr(B), _ptr(X), C.byref(o), reps, int(dev),
+                              C.c_void_p(stream) if stream else None)
+        out = [r.as_dict() for r in reps]
+        if st != _lib.MF_SUCCESS:
+            err = MFError(st, "mf_solve_multi")
+            err.report = out
+            raise err
+        return X, out
+
     def spmv(self, x, y=None, precision="fp64", stream=None):
         L = _lib.load()
         dev = _is_cuda_tensor(x)

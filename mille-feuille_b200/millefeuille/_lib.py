@@ -91,6 +91,7 @@ def load() -> C.CDLL:
     L.mf_spmv.argtypes = [vp, vp, vp, C.c_int, C.c_int, vp, dp]
     L.mf_spmv_noalloc.argtypes = [vp, vp, vp, C.c_int, vp]
     L.mf_value_grad.argtypes = [vp, C.c_int, vp, vp, vp, C.c_int, vp]
+    L.mf_solve_multi.argtypes = [vp, C.c_int, vp, vp, C.POINTER(Options), C.POINTER(Report), C.c_int, vp]
     L.mf_matrix_create_transposed.argtypes = [C.POINTER(vp), vp, vp]
     L.mf_debug_ref_labels.argtypes = [vp, vp, C.c_int, vp, C.c_int]
     L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]

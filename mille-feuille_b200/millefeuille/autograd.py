@@ -4,8 +4,8 @@ and for A's stored values.
     x = sparse_solve(rowptr, colidx, val, b, method="cg", precision="mixed")
     loss(x).backward()        # fills val.grad and b.grad
 
-Forward: one single-kernel solve per right-hand side (mf_solve on device
-pointers).  Backward: the adjoint solve lambda = A^-T dL/dx with the same
+Forward: the single-kernel solve on device pointers (mf_solve_multi, up to 8
+right-hand sides per launch, for CG; one mf_solve per column for BiCGSTAB).  Backward: the adjoint solve lambda = A^-T dL/dx with the same
 kernel -- on A itself for CG (A symmetric), on a transposed handle
 (mf_matrix_create_transposed) for BiCGSTAB -- then dL/db = lambda and
 dL/dval[e] = -sum_k lambda_k[i] x_k[j] over A's stored pattern (mf_value_grad,
@@ -54,7 +54,13 @@ class SolvePattern:
 
 
 def _solve_all(A: Matrix, B, opts, reports):
+    """All right-hand sides: mf_solve_multi (up to 8 per launch) for CG in the
+    FP64 / mixed modes, one mf_solve per column otherwise."""
     X = torch.zeros_like(B)
+    if B.shape[0] > 1 and opts.method == 0 and opts.precision in (0, 1):
+        _, reps = A.solve_multi(B, X, options=opts)
+        reports.extend(reps)
+        return X
     for k in range(B.shape[0]):
         _, rep = A.solve(B[k], X[k], options=opts)
         reports.append(rep)
