@@ -3,8 +3,10 @@
     python mille-feuille_b200/build.py [--verbose]
 
 Object files go to mille-feuille_b200/_build/, the shared library to
-mille-feuille_b200/millefeuille/libmillefeuille.so (git-ignored, carried with
-the tree).  Rebuilds only what changed.
+mille-feuille_b200/millefeuille/libmillefeuille.so and the drop-in driver
+executables (main-cg, main-cg-mixed, main-bicg, main-bicg-mixed) to
+mille-feuille_b200/bin/ (all git-ignored, carried with the tree).  Rebuilds
+only what changed.
 """
 from __future__ import annotations
 
@@ -47,19 +49,42 @@ def build(verbose: bool = False) -> str:
         if verbose and src.endswith(".cu"):
             cmd += ["-Xptxas", "-v"]
         if src.endswith(".cpp"):
-            cmd = ["g++", "-O2", "-fPIC", "-std=c++17", "-I", INCLUDE, "-c", sp, "-o", obj]
+            cmd = ["g++", "-O2", "-fPIC", "-pthread", "-std=c++17", "-I", INCLUDE, "-c", sp, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
         if r.returncode:
             raise RuntimeError(f"compile failed: {src}")
     if any(_newer(o, OUT, []) for o in objs) or not os.path.exists(OUT):
-        cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart", "-Xcompiler", "-pthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError("link failed")
+    build_drivers(verbose)
     return OUT
+
+
+DRIVERS = ["main-cg", "main-cg-mixed", "main-bicg", "main-bicg-mixed"]
+BIN = os.path.join(HERE, "bin")
+
+
+def build_drivers(verbose: bool = False) -> None:
+    """The reference's four benchmark executables over the library
+    (csrc/driver_main.cpp, variant chosen by MF_DRIVER) into bin/."""
+    os.makedirs(BIN, exist_ok=True)
+    src = os.path.join(CSRC, "driver_main.cpp")
+    for k, name in enumerate(DRIVERS):
+        exe = os.path.join(BIN, name)
+        if not _newer(src, exe, [OUT, os.path.join(INCLUDE, "millefeuille.h")]):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", f"-DMF_DRIVER={k}", "-I", INCLUDE, src, "-o", exe,
+               "-L", os.path.dirname(OUT), "-lmillefeuille", "-Wl,-rpath,$ORIGIN/../millefeuille"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or r.returncode:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode:
+            raise RuntimeError(f"driver build failed: {name}")
 
 
 if __name__ == "__main__":

@@ -3,7 +3,8 @@
 // mmio_highlevel.h:151-323): 1-based -> 0-based, entries placed in file order,
 // symmetric / hermitian entries mirrored (diagonal once), pattern -> 1.0,
 // integer -> its value, complex -> real part.  The whole file is read at once
-// and tokenised in memory (the reference parses with fscanf).
+// and parsed in memory by all host threads (the reference parses serially
+// with fscanf); the result is identical to a serial pass.
 #include "../../include/millefeuille.h"
 
 #include <cctype>
@@ -11,7 +12,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace {
@@ -43,6 +46,53 @@ inline void skip_ws(const char *&p)
     while (*p && isspace((unsigned char)*p)) p++;
 }
 
+// One chunk of coordinate lines [beg, end), parsed into (row, col, value) in
+// file order.  Returns false on a malformed or out-of-range entry.
+struct Chunk {
+    std::vector<int> ri, ci;
+    std::vector<double> vv;
+    bool ok = true;
+};
+
+void parse_chunk(const char *beg, const char *end, long long M, long long N, bool real, bool complex_,
+                 bool integer, Chunk &out)
+{
+    const char *q = beg;
+    char *e = nullptr;
+    while (q < end) {
+        while (q < end && isspace((unsigned char)*q)) q++;
+        if (q >= end) break;
+        const long long a = strtoll(q, &e, 10);
+        if (e == q) { out.ok = false; return; }
+        q = e;
+        const long long c = strtoll(q, &e, 10);
+        if (e == q) { out.ok = false; return; }
+        q = e;
+        double v = 1.0;
+        if (real || complex_) {
+            v = strtod(q, &e);
+            if (e == q) { out.ok = false; return; }
+            q = e;
+            if (complex_) { strtod(q, &e); q = e; }
+        } else if (integer) {
+            v = (double)(int)strtol(q, &e, 10);
+            if (e == q) { out.ok = false; return; }
+            q = e;
+        }
+        if (a < 1 || a > M || c < 1 || c > N) { out.ok = false; return; }
+        out.ri.push_back((int)(a - 1));
+        out.ci.push_back((int)(c - 1));
+        out.vv.push_back(v);
+        while (q < end && *q != '\n') q++;     // rest of the line (imaginary part etc.)
+    }
+}
+
+// Matrix Market coordinate file -> 0-based CSR.  The data lines are cut into
+// chunks at line boundaries and parsed by one host thread each; every thread
+// then counts its entries per row (mirrored ones included), the per-row
+// offsets are the prefix over (row, chunk), and each thread places its entries
+// in its own order -- so a row's entries stay in file order, exactly as a
+// serial pass places them (a mirrored entry at the position of its line).
 int read_mtx(const char *path, int *m, int *n, int *nnz, int **rowptr, int **colidx, double **val, int *is_sym)
 {
     std::vector<char> buf;
@@ -73,57 +123,77 @@ int read_mtx(const char *path, int *m, int *n, int *nnz, int **rowptr, int **col
     long long N = strtoll(q, &end, 10); q = end;
     long long NZ = strtoll(q, &end, 10); q = end;
     if (M <= 0 || N <= 0 || NZ < 0 || M > INT32_MAX || N > INT32_MAX) return MF_ERR_IO;
-    std::vector<int> ri((size_t)NZ), ci((size_t)NZ);
-    std::vector<double> vv((size_t)NZ);
-    std::vector<long long> cnt((size_t)M + 1, 0);
-    for (long long k = 0; k < NZ; k++) {
-        skip_ws(q);
-        long long a = strtoll(q, &end, 10);
-        if (end == q) return MF_ERR_IO;
-        q = end;
-        long long c = strtoll(q, &end, 10);
-        if (end == q) return MF_ERR_IO;
-        q = end;
-        double v = 1.0;
-        if (real || complex_) {
-            v = strtod(q, &end);
-            if (end == q) return MF_ERR_IO;
-            q = end;
-            if (complex_) { strtod(q, &end); q = end; }
-        } else if (integer) {
-            v = (double)(int)strtol(q, &end, 10);
-            if (end == q) return MF_ERR_IO;
-            q = end;
-        }
-        if (a < 1 || a > M || c < 1 || c > N) return MF_ERR_IO;
-        ri[k] = (int)(a - 1);
-        ci[k] = (int)(c - 1);
-        vv[k] = v;
-        cnt[(size_t)(a - 1)]++;
+    while (*q && *q != '\n') q++;               // end of the size line
+    const char *data = q, *data_end = buf.data() + buf.size() - 1;
+
+    // chunks at line boundaries, one per thread
+    const size_t bytes = (size_t)(data_end - data);
+    unsigned hw = std::thread::hardware_concurrency();
+    int T = (int)std::min<size_t>(std::max(1u, std::min(hw, 64u)), bytes / (1u << 20) + 1);
+    std::vector<const char *> cut(T + 1);
+    cut[0] = data;
+    cut[T] = data_end;
+    for (int k = 1; k < T; k++) {
+        const char *c = data + bytes * k / T;
+        if (c < cut[k - 1]) c = cut[k - 1];
+        while (c < data_end && *c != '\n') c++;
+        cut[k] = c;
     }
-    if (sym)
-        for (long long k = 0; k < NZ; k++)
-            if (ri[k] != ci[k]) cnt[(size_t)ci[k]]++;
-    std::vector<long long> start((size_t)M + 1, 0);
-    for (long long i = 0; i < M; i++) start[i + 1] = start[i] + cnt[i];
-    const long long total = start[M];
-    if (total > INT32_MAX) return MF_ERR_UNSUPPORTED;
+    std::vector<Chunk> ch(T);
+    auto run = [&](auto &&fn) {
+        std::vector<std::thread> th;
+        for (int k = 1; k < T; k++) th.emplace_back(fn, k);
+        fn(0);
+        for (auto &x : th) x.join();
+    };
+    run([&](int k) { parse_chunk(cut[k], cut[k + 1], M, N, real, complex_, integer, ch[k]); });
+    long long got = 0;
+    for (auto &c : ch) {
+        if (!c.ok) return MF_ERR_IO;
+        got += (long long)c.ri.size();
+    }
+    if (got != NZ) return MF_ERR_IO;
+
+    // per-chunk row counts, then offsets in (row, chunk) order
+    std::vector<std::vector<int>> cnt(T);
+    run([&](int k) {
+        cnt[k].assign((size_t)M, 0);
+        const Chunk &c = ch[k];
+        for (size_t e = 0; e < c.ri.size(); e++) {
+            cnt[k][c.ri[e]]++;
+            if (sym && c.ri[e] != c.ci[e]) cnt[k][c.ci[e]]++;
+        }
+    });
     int *rp = (int *)malloc(sizeof(int) * (size_t)(M + 1));
+    if (!rp) return MF_ERR_NOMEM;
+    long long total = 0;
+    for (long long i = 0; i < M; i++) {
+        rp[i] = (int)std::min<long long>(total, INT32_MAX);
+        for (int k = 0; k < T; k++) {
+            const int c = cnt[k][i];
+            cnt[k][i] = (int)std::min<long long>(total, INT32_MAX);   // becomes chunk k's cursor in row i
+            total += c;
+        }
+    }
+    if (total > INT32_MAX) { free(rp); return MF_ERR_UNSUPPORTED; }
+    rp[M] = (int)total;
     int *cc = (int *)malloc(sizeof(int) * (size_t)(total > 0 ? total : 1));
     double *vo = (double *)malloc(sizeof(double) * (size_t)(total > 0 ? total : 1));
-    if (!rp || !cc || !vo) { free(rp); free(cc); free(vo); return MF_ERR_NOMEM; }
-    for (long long i = 0; i <= M; i++) rp[i] = (int)start[i];
-    std::vector<long long> fill(start.begin(), start.end() - 1);
-    for (long long k = 0; k < NZ; k++) {
-        long long o = fill[(size_t)ri[k]]++;
-        cc[o] = ci[k];
-        vo[o] = vv[k];
-        if (sym && ri[k] != ci[k]) {
-            o = fill[(size_t)ci[k]]++;
-            cc[o] = ri[k];
-            vo[o] = vv[k];
+    if (!cc || !vo) { free(rp); free(cc); free(vo); return MF_ERR_NOMEM; }
+    run([&](int k) {
+        const Chunk &c = ch[k];
+        std::vector<int> &cur = cnt[k];
+        for (size_t e = 0; e < c.ri.size(); e++) {
+            int o = cur[c.ri[e]]++;
+            cc[o] = c.ci[e];
+            vo[o] = c.vv[e];
+            if (sym && c.ri[e] != c.ci[e]) {
+                o = cur[c.ci[e]]++;
+                cc[o] = c.ri[e];
+                vo[o] = c.vv[e];
+            }
         }
-    }
+    });
     *m = (int)M; *n = (int)N; *nnz = (int)total;
     *rowptr = rp; *colidx = cc; *val = vo; *is_sym = sym ? 1 : 0;
     return MF_SUCCESS;

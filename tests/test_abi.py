@@ -79,6 +79,32 @@ def test_mtx_reader_matches_oracle_and_reference(mf, oracle_mod, tmp_path, field
             np.testing.assert_array_equal(g, e)
 
 
+@pytest.mark.parametrize("sym", [False, True])
+def test_mtx_reader_parallel_chunks_keep_file_order(mf, oracle_mod, tmp_path, sym):
+    """A file of several MB is parsed in line-aligned chunks by several host
+    threads; entries shuffled in the file (and mirrored ones) must land in
+    file order within each row, as the serial oracle places them."""
+    rng = np.random.default_rng(12)
+    n, nz = 20000, 300000
+    r = rng.integers(1, n + 1, nz)
+    c = rng.integers(1, n + 1, nz)
+    if sym:
+        r, c = np.maximum(r, c), np.minimum(r, c)
+    v = rng.standard_normal(nz)
+    path = tmp_path / "big.mtx"
+    with open(path, "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real {'symmetric' if sym else 'general'}\n")
+        f.write("% comment line\n")
+        f.write(f"{n} {n} {nz}\n")
+        f.write("".join(f"{a} {b} {x!r}\n" for a, b, x in zip(r.tolist(), c.tolist(), v.tolist())))
+    assert path.stat().st_size > 4 << 20
+    got = mf.read_matrix(str(path))
+    exp = oracle_mod.read_mtx(str(path))
+    assert got[:2] == exp[:2] and got[5] == exp[5]
+    for g, e in zip(got[2:5], exp[2:5]):
+        np.testing.assert_array_equal(g, e)
+
+
 def test_cbd_roundtrip(mf, tmp_path):
     from millefeuille import matrices as M
     A = M.random_csr(50, 60, 0.1, seed=6)
