@@ -208,6 +208,34 @@ int mf_solve(mf_matrix A, const double *b, double *x, const mf_options *opt, mf_
 int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_options *opt,
                    mf_report *reports, int device_ptrs, void *stream);
 
+/*
+ * Batched solves: many independent square systems (each an mf_matrix on the
+ * current device) with nrhs[k] right-hand sides each, in ONE persistent launch.
+ * A device work queue holds (system, up to `cap` right-hand sides) items,
+ * largest estimated cost first; each 512-thread block takes the next item and
+ * solves it alone (CG, FP64 or mixed; block-level syncs), then the next.  No
+ * counterpart in the reference (one system per call).
+ *
+ * mf_batch_create  keeps the handles' pointers (the matrices must outlive the
+ *                  batch) and sizes the work items (cap 8).
+ * mf_batch_tune    picks the right-hand sides per item (8, 4 or 2) by timing
+ *                  `iters` fixed iterations of the real batch; *chosen_cap
+ *                  (nullable) gets the choice.
+ * mf_batch_solve   B[k] / X[k]: DEVICE arrays of nrhs[k] x n_k doubles (one
+ *                  vector after another).  reports (nullable): sum(nrhs)
+ *                  records, system by system; time_ms is the whole batch's.
+ *                  use_graph != 0: the enqueue sequence (interleave, queue
+ *                  reset, launch, de-interleave) is captured into a CUDA graph
+ *                  on first use and replayed while the pointers and options stay
+ *                  the same.  stream NULL: the batch's own stream.
+ */
+typedef struct mf_batch_s *mf_batch;
+int mf_batch_create(mf_batch *out, int nsys, const mf_matrix *systems, const int *nrhs, void *stream);
+int mf_batch_tune(mf_batch b, int precision, int iters, int *chosen_cap, void *stream);
+int mf_batch_solve(mf_batch b, const double *const *B, double *const *X, const mf_options *opt,
+                   mf_report *reports, int use_graph, void *stream);
+int mf_batch_destroy(mf_batch b);
+
 /* y = A x with the tile kernel.  precision: MF_PREC_FP64 or MF_PREC_MIXED
  * (MIXED here means every tile in FP32).  elapsed_ms (nullable) gets the kernel time. */
 int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs,

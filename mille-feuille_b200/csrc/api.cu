@@ -334,6 +334,37 @@ extern "C" int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X,
     return rc;
 }
 
+extern "C" int mf_batch_create(mf_batch *out, int nsys, const mf_matrix *systems, const int *nrhs, void *stream)
+{
+    if (!out || nsys < 1 || !systems || !nrhs) return MF_ERR_INVALID;
+    *out = nullptr;
+    MF_TRY(device_ready());
+    return mf_batch_create_impl(out, nsys, systems, nrhs, (cudaStream_t)stream);
+}
+
+extern "C" int mf_batch_tune(mf_batch b, int precision, int iters, int *chosen_cap, void *stream)
+{
+    if (!b || iters < 1 || (precision != MF_PREC_FP64 && precision != MF_PREC_MIXED)) return MF_ERR_INVALID;
+    return mf_batch_tune_impl(b, precision, iters, chosen_cap, (cudaStream_t)stream);
+}
+
+extern "C" int mf_batch_solve(mf_batch b, const double *const *B, double *const *X, const mf_options *opt,
+                              mf_report *reports, int use_graph, void *stream)
+{
+    if (!b || !B || !X) return MF_ERR_INVALID;
+    mf_options o;
+    if (opt) o = *opt;
+    else mf_options_default(&o);
+    return mf_batch_solve_impl(b, B, X, &o, reports, use_graph, (cudaStream_t)stream);
+}
+
+extern "C" int mf_batch_destroy(mf_batch b)
+{
+    if (!b) return MF_ERR_INVALID;
+    mf_batch_destroy_impl(b);
+    return MF_SUCCESS;
+}
+
 extern "C" int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs, void *stream,
                        double *elapsed_ms)
 {

@@ -115,6 +115,11 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
                   mf_report *rep, cudaStream_t s);
 int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X, const mf_options *opt,
                         mf_report *reps, cudaStream_t s);
+int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems, const int *nrhs, cudaStream_t s);
+int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *Xd, const mf_options *opt,
+                        mf_report *reps, int use_graph, cudaStream_t s);
+int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cudaStream_t s);
+void mf_batch_destroy_impl(mf_batch_s *b);
 int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s,
                 double *elapsed_ms);
 int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s);

@@ -18,6 +18,7 @@
 //  * matrix payload is streamed with evict-first loads so the vectors stay in L2.
 #include "mf_internal.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -589,6 +590,19 @@ struct PhaseClock {
 };
 enum { PH_SPMV = 0, PH_VECB = 1, PH_VECC = 2, PH_BAR = 3, PH_REPL = 4 };
 
+// After an FP64 residual replacement r = b - A x: keep the CG direction only
+// while the recursive residual still told the truth.  When the replacement
+// follows a failed convergence check (the recursive residual claimed
+// convergence, the true one did not) or the two squared norms differ by more
+// than 4x, the recursive residual has drifted to the accuracy floor of the
+// low-precision products; beta = r_true.r_true / r_old.r_old would then be
+// meaningless (huge when r_old has collapsed), so CG restarts from the true
+// residual (beta = 0, which also makes q = A p consistent again).
+__device__ __forceinline__ bool restart_after_replacement(bool failed_check, double rr_true, double rr_rec)
+{
+    return failed_check || rr_true > 4.0 * rr_rec || 4.0 * rr_true < rr_rec;
+}
+
 template <int MODE, int LB>
 __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
 {
@@ -721,11 +735,13 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             grid_collect(P, sh, 2, 2, 0x2u, v);
             clk.lap(PH_BAR);
             double rr_new = v[0];
+            const double rr_rec = rr_new;       // recursive r.r of this iteration
             invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
             k++;
             last_true = 0;
             const bool want_check = !P.fixed_iters && rr_new <= thr2;
             const bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
+            bool restart = false;
             if (want_check || want_repl) {
                 // ---- FP64 true residual r = b - A x (x is current), r's shadow ----
                 double prt = 0.0;
@@ -768,8 +784,9 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 repl++;
                 last_true = 1;
                 if (!P.fixed_iters && rr_new <= thr2) { rr = rr_new; conv = 1; break; }
+                restart = restart_after_replacement(want_check, rr_new, rr_rec);
             }
-            beta2 = rr_new / rr;
+            beta2 = restart ? 0.0 : rr_new / rr;
             rr = rr_new;
             continue;
         }
@@ -900,11 +917,13 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             clk.lap(PH_BAR);
         }
         double rr_new = v[0], r1_new = bicg ? v[1] : 0.0;
+        const double rr_rec = rr_new;    // recursive r.r of this iteration
         k++;
         last_true = 0;
         bool x_done = bicg;      // CG defers x += alpha p to phase C
         const bool want_check = !P.fixed_iters && rr_new <= thr2;
         const bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
+        bool restart = false;
         if (want_check || want_repl) {
             if (!x_done) {
                 // the FP64 residual needs the current x: apply this iteration's step first
@@ -948,10 +967,16 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             repl++;
             last_true = 1;
             if (!P.fixed_iters && rr_new <= thr2) { rr = rr_new; conv = 1; break; }
+            restart = restart_after_replacement(want_check, rr_new, rr_rec);
         }
         // ---- C: (CG: x += alpha p,) p = r + beta p  /  p = r + beta (p - omega v) ----
+        // A restart (see restart_after_replacement) takes p = r; BiCGSTAB also
+        // takes the true residual as its new shadow residual (rh = r, r1 = r.r).
         double beta;
-        if (!bicg) {
+        if (restart) {
+            beta = 0.0;
+            if (bicg) r1 = rr_new;
+        } else if (!bicg) {
             beta = rr_new / rr;
         } else {
             beta = (r1_new * alpha) / (r1 * omega);
@@ -981,6 +1006,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 if (valid) {
                     if (!bicg && !x_done) P.x[row] = xq[u] + alpha * pold;
                     P.p[row] = pn;
+                    if (bicg && restart) P.rh[row] = rv[u];
                 }
                 publish_dir<MODE>(R, row, valid, valid ? pn : 0.0, pold, P.p32, P.p16, P.p8, P.mag_p, P.lab_p,
                                   bmax, c.hmask, true);
@@ -1221,12 +1247,16 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
                     const int xi = __shfl_sync(hmask, xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
                     if (k0 + j < len) {
                         const double v = __ldcs(P.v64 + off + (long long)(k0 + j) * MF_BS + i);
-                        const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
+                        if constexpr (NR == 1) {
+                            acc[0] = fma(v, X64[xi], acc[0]);
+                        } else {
+                            const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
 #pragma unroll
-                        for (int q = 0; q < NR / 2; q++) {
-                            const double2 d = xr[q];
-                            acc[2 * q] = fma(v, d.x, acc[2 * q]);
-                            acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
+                            for (int q = 0; q < NR / 2; q++) {
+                                const double2 d = xr[q];
+                                acc[2 * q] = fma(v, d.x, acc[2 * q]);
+                                acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
+                            }
                         }
                     }
                 }
@@ -1245,12 +1275,16 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
                         const float v = (pr == MF_P32)   ? __ldcs(P.v32 + e)
                                         : (pr == MF_P16) ? __half2float(P.v16[e])
                                                          : (float)P.v8[e] * s8;
-                        const float2 *xr = (const float2 *)(X32 + (long long)xi * NR);
+                        if constexpr (NR == 1) {
+                            part[0] = fmaf(v, X32[xi], part[0]);
+                        } else {
+                            const float2 *xr = (const float2 *)(X32 + (long long)xi * NR);
 #pragma unroll
-                        for (int q = 0; q < NR / 2; q++) {
-                            const float2 d = xr[q];
-                            part[2 * q] = fmaf(v, d.x, part[2 * q]);
-                            part[2 * q + 1] = fmaf(v, d.y, part[2 * q + 1]);
+                            for (int q = 0; q < NR / 2; q++) {
+                                const float2 d = xr[q];
+                                part[2 * q] = fmaf(v, d.x, part[2 * q]);
+                                part[2 * q + 1] = fmaf(v, d.y, part[2 * q + 1]);
+                            }
                         }
                     }
                 }
@@ -1283,11 +1317,16 @@ __device__ __forceinline__ void publish_multi(const MultiParams &M, int R, int r
     if (MODE != MODE_MIXED) return;
     float m = 0.0f;
     if (valid) {
-        float2 *dst = (float2 *)(M.R32 + (long long)row * NR);
+        if constexpr (NR == 1) {
+            M.R32[row] = (float)rv[0];
+            m = fabsf((float)rv[0]);
+        } else {
+            float2 *dst = (float2 *)(M.R32 + (long long)row * NR);
 #pragma unroll
-        for (int q = 0; q < NR / 2; q++) {
-            dst[q] = make_float2((float)rv[2 * q], (float)rv[2 * q + 1]);
-            m = fmaxf(m, fmaxf(fabsf((float)rv[2 * q]), fabsf((float)rv[2 * q + 1])));
+            for (int q = 0; q < NR / 2; q++) {
+                dst[q] = make_float2((float)rv[2 * q], (float)rv[2 * q + 1]);
+                m = fmaxf(m, fmaxf(fabsf((float)rv[2 * q]), fabsf((float)rv[2 * q + 1])));
+            }
         }
     }
     m = half_max(m, hmask);
@@ -1299,6 +1338,10 @@ __device__ __forceinline__ void publish_multi(const MultiParams &M, int R, int r
 template <int NR>
 __device__ __forceinline__ void load_row(const double *v, int row, double (&out)[NR])
 {
+    if constexpr (NR == 1) {
+        out[0] = v[row];
+        return;
+    }
     const double2 *p = (const double2 *)(v + (long long)row * NR);
 #pragma unroll
     for (int q = 0; q < NR / 2; q++) {
@@ -1310,17 +1353,20 @@ __device__ __forceinline__ void load_row(const double *v, int row, double (&out)
 template <int NR>
 __device__ __forceinline__ void store_row(double *v, int row, const double (&in)[NR])
 {
+    if constexpr (NR == 1) {
+        v[row] = in[0];
+        return;
+    }
     double2 *p = (double2 *)(v + (long long)row * NR);
 #pragma unroll
     for (int q = 0; q < NR / 2; q++) p[q] = make_double2(in[2 * q], in[2 * q + 1]);
 }
 
-template <int MODE, int NR>
-__global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, MultiParams M)
+// The CG iterations on NR columns, generic in how the threads that share a
+// system synchronise: the whole grid (k_solve_multi) or one block (k_batch).
+template <int MODE, int NR, class Sync>
+__device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const Ctx &c, SharedM &sh, Sync &sy)
 {
-    __shared__ SharedM sh;
-    const Ctx c = make_ctx(P);
-    unsigned epoch = 0;
     const int n = P.n;
     bool has_empty = false;
     for (int R = c.rbeg; R < c.rend && !has_empty; R++) has_empty = P.seg_ptr[R] == P.seg_ptr[R + 1];
@@ -1350,10 +1396,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
     }
     pb[NR] = st.mx;
     pb[NR + 1] = -st.mn;
-    block_partial_m<NR + 2>(M, sh, 0, pb, mm2);
-    if (!grid_barrier(P, epoch, sh)) return;
     double v[NR + 2];
-    grid_collect_m<NR + 2>(M, sh, 0, mm2, v);
+    if (!sy.template reduce<NR + 2>(0, pb, mm2, v)) return;
     if (threadIdx.x == 0) {
         for (int k = 0; k < NR; k++) {
             sh.bb[k] = v[k];
@@ -1408,10 +1452,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
             for (int R = c.rbeg; R < c.rend; R++)
                 if (P.seg_ptr[R] == P.seg_ptr[R + 1]) upd_a(R, zw);
         }
-        block_partial_m<NR>(M, sh, 1, ppq, 0u);
-        if (!grid_barrier(P, epoch, sh)) return;
         double pq[NR];
-        grid_collect_m<NR>(M, sh, 1, 0u, pq);
+        if (!sy.template reduce<NR>(1, ppq, 0u, pq)) return;
         if (threadIdx.x == 0) {
             for (int j = 0; j < NR; j++) {
                 double a = sh.active[j] ? sh.rr[j] / pq[j] : 0.0;
@@ -1455,9 +1497,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
         }
         prr[NR] = st.mx;
         prr[NR + 1] = -st.mn;
-        block_partial_m<NR + 2>(M, sh, 2, prr, mm2);
-        if (!grid_barrier(P, epoch, sh)) return;
-        grid_collect_m<NR + 2>(M, sh, 2, mm2, v);
+        if (!sy.template reduce<NR + 2>(2, prr, mm2, v)) return;
         invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
         k++;
         last_true = 0;
@@ -1465,9 +1505,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
 #pragma unroll
         for (int j = 0; j < NR; j++)
             if (sh.active[j] && !P.fixed_iters && v[j] <= sh.thr2[j]) want_repl = true;
-        double rnew[NR];
+        double rnew[NR], rrec[NR];
 #pragma unroll
-        for (int j = 0; j < NR; j++) rnew[j] = v[j];
+        for (int j = 0; j < NR; j++) rnew[j] = rrec[j] = v[j];
         if (want_repl) {
             // ---- FP64 R = B - A X, R's shadow, true residual norms ----
             double prt[NR + 2];
@@ -1501,9 +1541,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
             }
             prt[NR] = st.mx;
             prt[NR + 1] = -st.mn;
-            block_partial_m<NR + 2>(M, sh, 5, prt, mm2);
-            if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect_m<NR + 2>(M, sh, 5, mm2, v);
+            if (!sy.template reduce<NR + 2>(5, prt, mm2, v)) return;
             invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
             repl++;
             last_true = 1;
@@ -1520,7 +1558,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
                     sh.conv[j] = 1;
                     sh.iters[j] = k;
                 }
-                sh.beta[j] = sh.active[j] ? rnew[j] / sh.rr[j] : 0.0;
+                const bool restart = last_true &&
+                                     restart_after_replacement(!P.fixed_iters && rrec[j] <= sh.thr2[j], rnew[j], rrec[j]);
+                sh.beta[j] = (sh.active[j] && !restart) ? rnew[j] / sh.rr[j] : 0.0;
                 if (sh.active[j] || !sh.conv[j]) sh.rr[j] = rnew[j];
             }
         }
@@ -1548,14 +1588,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
             for (int R = c.rbeg; R < c.rend; R++)
                 if (P.seg_ptr[R] == P.seg_ptr[R + 1]) acc_r(R, zy);
         }
-        block_partial_m<NR>(M, sh, 7, prt, 0u);
-        if (!grid_barrier(P, epoch, sh)) return;
         double w[NR];
-        grid_collect_m<NR>(M, sh, 7, 0u, w);
+        if (!sy.template reduce<NR>(7, prt, 0u, w)) return;
 #pragma unroll
         for (int j = 0; j < NR; j++) rt[j] = w[j];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (sy.writer()) {
         for (int j = 0; j < NR; j++) {
             const double bb = sh.bb[j];
             M.out[4 * j + 0] = (double)(sh.conv[j] ? sh.iters[j] : k);
@@ -1566,6 +1604,178 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
         M.out[4 * NR + 0] = (double)k;
         M.out[4 * NR + 1] = (double)status;
         M.out[4 * NR + 2] = (double)repl;
+    }
+}
+
+// Grid-wide synchronisation: block partials, the counter barrier, a fixed-order collect.
+struct GridSync {
+    const SolverParams &P;
+    const MultiParams &M;
+    SharedM &sh;
+    unsigned epoch;
+    template <int NV>
+    __device__ bool reduce(int kind, const double (&v)[NV], unsigned maxmask, double (&out)[NV])
+    {
+        block_partial_m<NV>(M, sh, kind, v, maxmask);
+        if (!grid_barrier(P, epoch, sh)) return false;
+        grid_collect_m<NV>(M, sh, kind, maxmask, out);
+        return true;
+    }
+    __device__ bool writer() const { return blockIdx.x == 0 && threadIdx.x == 0; }
+};
+
+template <int MODE, int NR>
+__global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, MultiParams M)
+{
+    __shared__ SharedM sh;
+    const Ctx c = make_ctx(P);
+    GridSync sy{P, M, sh, 0u};
+    cg_multi_body<MODE, NR>(P, M, c, sh, sy);
+}
+
+// ------------------------------------------------------------ batched systems
+// Many independent systems in one persistent launch.  A device work queue holds
+// (system, up to 8 of its right-hand sides) items, largest estimated cost first;
+// every block takes the next item, solves it alone with the CG body above --
+// block-level syncs instead of grid syncs, so the launch needs no co-residency
+// and can be captured in a CUDA graph -- and then takes the next one.
+constexpr int kHalvesPerBlock = kWarps * 2;
+
+struct BatchItem {
+    const int *seg_ptr;
+    const int4 *seg_hdr;
+    const int *seg_tile;
+    const uint16_t *seg_rowlen;
+    const unsigned char *meta;
+    const double *v64;
+    const float *v32;
+    const __half *v16;
+    const int8_t *v8;
+    const float *i8_scale;
+    const long long *row_cost;    // tile-row cost prefix [tilem + 1]
+    MultiParams M;                // the item's interleaved vectors and report words (M.nr columns used)
+    int n, tilem, nr;             // nr: interleave width (1, 2, 4 or 8)
+};
+
+struct BatchParams {
+    const BatchItem *items;
+    const int *order;             // item indices, largest estimated cost first
+    int n_items;
+    unsigned *head;               // next position in `order` (zeroed before the launch)
+    int max_iter, fixed_iters, replace_every, use_lossless;
+    double tol;
+    float demote16, demote8;
+};
+
+// One block's synchronisation: warp shuffles, shared memory, fixed order.
+struct BlockSync {
+    SharedM &sh;
+    template <int NV>
+    __device__ bool reduce(int, const double (&v)[NV], unsigned maxmask, double (&out)[NV])
+    {
+        const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double a = v[k];
+            const bool mx = (maxmask >> k) & 1u;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const double b = __shfl_xor_sync(0xffffffffu, a, o);
+                a = mx ? fmax(a, b) : a + b;
+            }
+            if (lane == 0) sh.wred[wib][k] = a;
+        }
+        __syncthreads();
+        if (wib < NV) {
+            const bool mx = (maxmask >> wib) & 1u;
+            double a = (lane < kWarps) ? sh.wred[lane][wib] : (mx ? -1.0e300 : 0.0);
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                const double b = __shfl_xor_sync(0xffffffffu, a, o);
+                a = mx ? fmax(a, b) : a + b;
+            }
+            if (lane == 0) sh.bcast[wib] = a;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < NV; k++) out[k] = sh.bcast[k];
+        __syncthreads();
+        return true;
+    }
+    __device__ bool writer() const { return threadIdx.x == 0; }
+};
+
+// The half-warps of one block split a system's tile-rows by the cost prefix.
+__device__ __forceinline__ Ctx block_ctx(const BatchItem &it)
+{
+    Ctx c;
+    c.lane = threadIdx.x & 31;
+    c.wib = threadIdx.x >> 5;
+    c.half = c.lane >> 4;
+    c.i = c.lane & 15;
+    c.hmask = 0xFFFFu << (16 * c.half);
+    const int hw = c.wib * 2 + c.half;
+    const long long total = it.row_cost[it.tilem];
+    auto split = [&](int h) -> int {
+        if (h >= kHalvesPerBlock) return it.tilem;
+        const long long target = (long long)((double)total * (double)h / (double)kHalvesPerBlock);
+        int lo = 0, hi = it.tilem;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (it.row_cost[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    c.rbeg = split(hw);
+    c.rend = split(hw + 1);
+    c.sbeg = it.seg_ptr[c.rbeg];
+    c.send = it.seg_ptr[c.rend];
+    return c;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
+{
+    __shared__ SharedM sh;
+    __shared__ int next;
+    for (;;) {
+        if (threadIdx.x == 0) next = (int)atomicAdd(B.head, 1u);
+        __syncthreads();
+        const int pos = next;
+        __syncthreads();
+        if (pos >= B.n_items) break;
+        const BatchItem &it = B.items[B.order[pos]];
+        SolverParams P;              // the fields the CG body and the slice walk read
+        P.n = it.n;
+        P.tilem = it.tilem;
+        P.seg_ptr = it.seg_ptr;
+        P.seg_hdr = it.seg_hdr;
+        P.seg_tile = it.seg_tile;
+        P.seg_rowlen = it.seg_rowlen;
+        P.meta = it.meta;
+        P.v64 = it.v64;
+        P.v32 = it.v32;
+        P.v16 = it.v16;
+        P.v8 = it.v8;
+        P.i8_scale = it.i8_scale;
+        P.max_iter = B.max_iter;
+        P.fixed_iters = B.fixed_iters;
+        P.replace_every = B.replace_every;
+        P.use_lossless = B.use_lossless;
+        P.tol = B.tol;
+        P.demote16 = B.demote16;
+        P.demote8 = B.demote8;
+        const Ctx c = block_ctx(it);
+        BlockSync sy{sh};
+        const MultiParams M = it.M;
+        switch (it.nr) {
+        case 1: cg_multi_body<MODE, 1>(P, M, c, sh, sy); break;
+        case 2: cg_multi_body<MODE, 2>(P, M, c, sh, sy); break;
+        case 4: cg_multi_body<MODE, 4>(P, M, c, sh, sy); break;
+        default: cg_multi_body<MODE, 8>(P, M, c, sh, sy); break;
+        }
+        __syncthreads();
     }
 }
 
@@ -2171,4 +2381,337 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
         }
     }
     return first_err;
+}
+
+// ------------------------------------------------------------ batched systems (host)
+namespace {
+
+struct BatchImpl {
+    int dev = 0, cap = 8, nitems = 0, nsm = 0;
+    std::vector<mf_matrix_s *> sys;
+    std::vector<int> nrhs;
+    // items: system, first column, columns, interleave width
+    std::vector<int> it_sys, it_col0, it_ncol, it_nr;
+    std::vector<BatchItem> h_items;
+    BatchItem *d_items = nullptr;
+    int *d_order = nullptr;
+    unsigned *d_head = nullptr;
+    char *d_pool = nullptr;
+    size_t pool_bytes = 0;
+    std::vector<size_t> out_off;       // offset of each item's report words in the pool
+    cudaStream_t own = nullptr;        // used when the caller passes the default stream
+    cudaGraphExec_t graph = nullptr;
+    std::vector<const void *> graph_key;
+    int graph_mode = -1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e_in = nullptr;
+    double last_ms = 0.0;
+
+    void release_items()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        graph_key.clear();
+        void *p[] = {d_items, d_order, d_head, d_pool};
+        for (void *q : p)
+            if (q) cudaFree(q);
+        d_items = nullptr; d_order = nullptr; d_head = nullptr; d_pool = nullptr;
+    }
+};
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr int kOutWords = 4 * kMaxNR + 8;
+
+// Items for column cap `cap`: each system's right-hand sides in groups of <= cap,
+// interleave width the next power of two (1, 2, 4, 8); all vectors in one pool.
+int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
+{
+    B.release_items();
+    B.cap = cap;
+    B.it_sys.clear(); B.it_col0.clear(); B.it_ncol.clear(); B.it_nr.clear();
+    for (int k = 0; k < (int)B.sys.size(); k++)
+        for (int c0 = 0; c0 < B.nrhs[k]; c0 += cap) {
+            const int g = std::min(cap, B.nrhs[k] - c0);
+            B.it_sys.push_back(k);
+            B.it_col0.push_back(c0);
+            B.it_ncol.push_back(g);
+            B.it_nr.push_back(g >= 5 ? 8 : g >= 3 ? 4 : g == 2 ? 2 : 1);
+        }
+    B.nitems = (int)B.it_sys.size();
+    // per item: B | X | R | P | Q (doubles), R32 (floats), segment magnitudes, report words
+    std::vector<size_t> off(B.nitems);
+    size_t total = 0;
+    B.out_off.assign(B.nitems, 0);
+    for (int t = 0; t < B.nitems; t++) {
+        const mf_matrix_s *A = B.sys[B.it_sys[t]];
+        const size_t L = (size_t)A->vec_len, nr = (size_t)B.it_nr[t];
+        off[t] = total;
+        total += align256(5 * L * nr * sizeof(double)) + align256(L * nr * sizeof(float)) +
+                 align256((size_t)(A->tilem + 1) * sizeof(float));
+        B.out_off[t] = total;
+        total += align256(kOutWords * sizeof(double));
+    }
+    B.pool_bytes = total;
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_pool, total > 0 ? total : 256));
+    MF_CUDA_TRY(cudaMemsetAsync(B.d_pool, 0, total > 0 ? total : 256, s));
+    B.h_items.resize(B.nitems);
+    std::vector<double> cost(B.nitems);
+    for (int t = 0; t < B.nitems; t++) {
+        const mf_matrix_s *A = B.sys[B.it_sys[t]];
+        const size_t L = (size_t)A->vec_len, nr = (size_t)B.it_nr[t];
+        BatchItem &it = B.h_items[t];
+        memset(&it, 0, sizeof(it));
+        it.seg_ptr = A->d_seg_ptr; it.seg_hdr = A->d_seg_hdr; it.seg_tile = A->d_seg_tile;
+        it.seg_rowlen = A->d_seg_rowlen; it.meta = A->d_meta; it.v64 = A->d_v64; it.v32 = A->d_v32;
+        it.v16 = A->d_v16; it.v8 = A->d_v8; it.i8_scale = A->d_i8_scale; it.row_cost = A->d_row_cost;
+        it.n = A->n_rows; it.tilem = A->tilem; it.nr = (int)nr;
+        char *base = B.d_pool + off[t];
+        double *v = (double *)base;
+        it.M.B = v; it.M.X = v + L * nr; it.M.R = v + 2 * L * nr; it.M.Pv = v + 3 * L * nr; it.M.Q = v + 4 * L * nr;
+        char *f = base + align256(5 * L * nr * sizeof(double));
+        it.M.R32 = (float *)f;
+        it.M.mag = (float *)(f + align256(L * nr * sizeof(float)));
+        it.M.red = nullptr;
+        it.M.out = (double *)(B.d_pool + B.out_off[t]);
+        it.M.nr = B.it_ncol[t];
+        // estimated work: entries x (widened) columns x iterations (~ sqrt(n) for these systems)
+        cost[t] = (double)A->nnz * (1.0 + 0.35 * (double)(nr - 1)) * std::sqrt((double)std::max(1, A->n_rows));
+    }
+    std::vector<int> order(B.nitems);
+    for (int t = 0; t < B.nitems; t++) order[t] = t;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_items, sizeof(BatchItem) * (size_t)std::max(1, B.nitems)));
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_order, sizeof(int) * (size_t)std::max(1, B.nitems)));
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_head, sizeof(unsigned)));
+    if (B.nitems > 0) {
+        MF_CUDA_TRY(cudaMemcpyAsync(B.d_items, B.h_items.data(), sizeof(BatchItem) * B.nitems,
+                                    cudaMemcpyHostToDevice, s));
+        MF_CUDA_TRY(cudaMemcpyAsync(B.d_order, order.data(), sizeof(int) * B.nitems, cudaMemcpyHostToDevice, s));
+    }
+    MF_CUDA_TRY(cudaStreamSynchronize(s));
+    return MF_SUCCESS;
+}
+
+// Enqueue one batched solve on s: interleave every item's columns, reset the
+// queue, the persistent launch, de-interleave.  No host synchronisation.
+int batch_enqueue(BatchImpl &B, const double *const *Bd, double *const *Xd, const BatchParams &bp0, int mode,
+                  cudaStream_t s)
+{
+    for (int t = 0; t < B.nitems; t++) {
+        const mf_matrix_s *A = B.sys[B.it_sys[t]];
+        const int nr = B.it_nr[t], g = B.it_col0[t] / nr;
+        k_interleave<<<148, 256, 0, s>>>(Bd[B.it_sys[t]], A->n_rows, A->vec_len, B.nrhs[B.it_sys[t]], g, nr,
+                                          (double *)B.h_items[t].M.B);
+    }
+    MF_CUDA_TRY(cudaGetLastError());
+    MF_CUDA_TRY(cudaMemsetAsync(B.d_head, 0, sizeof(unsigned), s));
+    BatchParams bp = bp0;
+    bp.items = B.d_items;
+    bp.order = B.d_order;
+    bp.n_items = B.nitems;
+    bp.head = B.d_head;
+    const int grid = std::max(1, std::min(B.nsm, B.nitems));
+    if (mode == MODE_FP64) k_batch<MODE_FP64><<<grid, kThreads, 0, s>>>(bp);
+    else k_batch<MODE_MIXED><<<grid, kThreads, 0, s>>>(bp);
+    MF_CUDA_TRY(cudaGetLastError());
+    for (int t = 0; t < B.nitems; t++) {
+        const mf_matrix_s *A = B.sys[B.it_sys[t]];
+        const int nr = B.it_nr[t], g = B.it_col0[t] / nr;
+        k_deinterleave<<<148, 256, 0, s>>>(B.h_items[t].M.X, A->n_rows, B.nrhs[B.it_sys[t]], g, nr,
+                                            Xd[B.it_sys[t]]);
+    }
+    MF_CUDA_TRY(cudaGetLastError());
+    return MF_SUCCESS;
+}
+
+}  // namespace
+
+struct mf_batch_s {
+    BatchImpl impl;
+};
+
+int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems, const int *nrhs, cudaStream_t s)
+{
+    mf_batch_s *b = new mf_batch_s();
+    BatchImpl &B = b->impl;
+    int rc = MF_SUCCESS;
+    if (cudaGetDevice(&B.dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&B.nsm, cudaDevAttrMultiProcessorCount, B.dev) != cudaSuccess)
+        rc = MF_ERR_CUDA;
+    for (int k = 0; rc == MF_SUCCESS && k < nsys; k++) {
+        if (!systems[k] || nrhs[k] < 1 || systems[k]->n_rows != systems[k]->n_cols || systems[k]->dev != B.dev) {
+            rc = MF_ERR_INVALID;
+            break;
+        }
+        B.sys.push_back(systems[k]);
+        B.nrhs.push_back(nrhs[k]);
+    }
+    if (rc == MF_SUCCESS &&
+        (cudaEventCreate(&B.e0) != cudaSuccess || cudaEventCreate(&B.e1) != cudaSuccess ||
+         cudaEventCreateWithFlags(&B.e_in, cudaEventDisableTiming) != cudaSuccess ||
+         cudaStreamCreateWithFlags(&B.own, cudaStreamNonBlocking) != cudaSuccess))
+        rc = MF_ERR_CUDA;
+    if (rc == MF_SUCCESS) rc = batch_build_items(B, 8, s ? s : B.own);
+    if (rc != MF_SUCCESS) {
+        mf_batch_destroy_impl(b);
+        return rc;
+    }
+    *out = b;
+    return MF_SUCCESS;
+}
+
+void mf_batch_destroy_impl(mf_batch_s *b)
+{
+    if (!b) return;
+    BatchImpl &B = b->impl;
+    B.release_items();
+    if (B.e0) cudaEventDestroy(B.e0);
+    if (B.e1) cudaEventDestroy(B.e1);
+    if (B.e_in) cudaEventDestroy(B.e_in);
+    if (B.own) cudaStreamDestroy(B.own);
+    delete b;
+}
+
+// Solve every system's right-hand sides.  Bd[k] / Xd[k]: device arrays of
+// nrhs[k] x n_k doubles.  With use_graph the sequence is captured into a CUDA
+// graph on first use and replayed while pointers, options and items stay the same.
+int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *Xd, const mf_options *opt,
+                        mf_report *reps, int use_graph, cudaStream_t s)
+{
+    BatchImpl &B = b->impl;
+    if (opt->method != MF_METHOD_CG || opt->precision == MF_PREC_PARITY || opt->x0_given) return MF_ERR_UNSUPPORTED;
+    const int mode = opt->precision == MF_PREC_FP64 ? MODE_FP64 : MODE_MIXED;
+    BatchParams bp;
+    memset(&bp, 0, sizeof(bp));
+    bp.max_iter = opt->max_iter;
+    bp.fixed_iters = opt->fixed_iters;
+    bp.replace_every = opt->replace_every;
+    bp.use_lossless = opt->use_lossless;
+    bp.tol = opt->tol;
+    bp.demote16 = (float)opt->demote_fp16;
+    bp.demote8 = (float)opt->demote_int8;
+    cudaStream_t run = s ? s : B.own;
+    if (!s) {
+        // the batch's own stream does not synchronise with the default stream on
+        // its own: order it after the work already queued there (inputs, zeroing)
+        MF_CUDA_TRY(cudaEventRecord(B.e_in, 0));
+        MF_CUDA_TRY(cudaStreamWaitEvent(B.own, B.e_in, 0));
+    }
+    if (use_graph) {
+        // the graph bakes in pointers, options and items: rebuilt when any changes
+        std::vector<const void *> key;
+        for (size_t k = 0; k < B.sys.size(); k++) {
+            key.push_back(Bd[k]);
+            key.push_back(Xd[k]);
+        }
+        const double opts[] = {opt->tol, (double)opt->max_iter, (double)opt->fixed_iters, (double)opt->replace_every,
+                               opt->demote_fp16, opt->demote_int8, (double)opt->use_lossless, (double)B.cap};
+        for (double v : opts) {
+            unsigned long long u;
+            memcpy(&u, &v, sizeof(u));
+            key.push_back((const void *)(uintptr_t)u);
+        }
+        if (!B.graph || key != B.graph_key || B.graph_mode != mode) {
+            if (B.graph) cudaGraphExecDestroy(B.graph);
+            B.graph = nullptr;
+            cudaGraph_t g = nullptr;
+            MF_CUDA_TRY(cudaStreamBeginCapture(run, cudaStreamCaptureModeThreadLocal));
+            const int rc = batch_enqueue(B, Bd, Xd, bp, mode, run);
+            const cudaError_t ce = cudaStreamEndCapture(run, &g);
+            if (rc != MF_SUCCESS) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            MF_CUDA_TRY(ce);
+            const cudaError_t ie = cudaGraphInstantiate(&B.graph, g, 0);
+            cudaGraphDestroy(g);
+            MF_CUDA_TRY(ie);
+            B.graph_key = key;
+            B.graph_mode = mode;
+        }
+        MF_CUDA_TRY(cudaEventRecord(B.e0, run));
+        MF_CUDA_TRY(cudaGraphLaunch(B.graph, run));
+        MF_CUDA_TRY(cudaEventRecord(B.e1, run));
+    } else {
+        MF_CUDA_TRY(cudaEventRecord(B.e0, run));
+        MF_TRY(batch_enqueue(B, Bd, Xd, bp, mode, run));
+        MF_CUDA_TRY(cudaEventRecord(B.e1, run));
+    }
+    std::vector<double> outs((size_t)B.nitems * kOutWords);
+    for (int t = 0; t < B.nitems; t++)
+        MF_CUDA_TRY(cudaMemcpyAsync(outs.data() + (size_t)t * kOutWords, B.d_pool + B.out_off[t],
+                                    kOutWords * sizeof(double), cudaMemcpyDeviceToHost, run));
+    MF_CUDA_TRY(cudaStreamSynchronize(run));
+    float ms = 0.f;
+    MF_CUDA_TRY(cudaEventElapsedTime(&ms, B.e0, B.e1));
+    B.last_ms = ms;
+    int status = MF_SUCCESS;
+    std::vector<int> first(B.sys.size() + 1, 0);
+    for (size_t k = 0; k < B.sys.size(); k++) first[k + 1] = first[k] + B.nrhs[k];
+    for (int t = 0; t < B.nitems; t++) {
+        const double *o = outs.data() + (size_t)t * kOutWords;
+        const int nr = B.it_nr[t];
+        if ((int)o[4 * nr + 1] != MF_SUCCESS && status == MF_SUCCESS) status = (int)o[4 * nr + 1];
+        if (!reps) continue;
+        for (int c = 0; c < B.it_ncol[t]; c++) {
+            mf_report *r = &reps[first[B.it_sys[t]] + B.it_col0[t] + c];
+            memset(r, 0, sizeof(*r));
+            r->iterations = (int)o[4 * c + 0];
+            r->converged = (int)o[4 * c + 1];
+            r->relres_true = o[4 * c + 2];
+            r->relres_rec = o[4 * c + 3];
+            r->status = (int)o[4 * nr + 1];
+            r->replacements = (int)o[4 * nr + 2];
+            r->time_ms = ms;
+            r->grid_blocks = std::max(1, std::min(B.nsm, B.nitems));
+            r->threads_per_block = kThreads;
+        }
+    }
+    return status;
+}
+
+// Right-hand sides per work item chosen by timing: each candidate cap runs
+// `iters` fixed iterations of the real batch with all-ones right-hand sides.
+int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cudaStream_t s)
+{
+    BatchImpl &B = b->impl;
+    cudaStream_t run = s ? s : B.own;
+    std::vector<double *> bufB(B.sys.size(), nullptr), bufX(B.sys.size(), nullptr);
+    int rc = MF_SUCCESS;
+    for (size_t k = 0; k < B.sys.size() && rc == MF_SUCCESS; k++) {
+        const size_t e = (size_t)B.nrhs[k] * B.sys[k]->n_rows;
+        if (cudaMalloc((void **)&bufB[k], 2 * e * sizeof(double) + 16) != cudaSuccess) {
+            rc = MF_ERR_NOMEM;
+            break;
+        }
+        bufX[k] = bufB[k] + e;
+        std::vector<double> ones(e, 1.0);
+        if (cudaMemcpy(bufB[k], ones.data(), e * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = MF_ERR_CUDA;
+    }
+    mf_options o;
+    mf_options_default(&o);
+    o.precision = precision;
+    o.fixed_iters = 1;
+    o.max_iter = iters;
+    o.replace_every = 0;
+    int best = 8;
+    double best_ms = 1e300;
+    for (int cap : {8, 4, 2}) {
+        if (rc != MF_SUCCESS) break;
+        if ((rc = batch_build_items(B, cap, run)) != MF_SUCCESS) break;
+        double ms = 0.0;
+        for (int rep = 0; rep < 2 && rc == MF_SUCCESS; rep++) {   // the first run warms up
+            rc = mf_batch_solve_impl(b, bufB.data(), bufX.data(), &o, nullptr, 0, run);
+            ms = B.last_ms;
+        }
+        if (rc == MF_SUCCESS && ms < best_ms) {
+            best_ms = ms;
+            best = cap;
+        }
+    }
+    for (size_t k = 0; k < B.sys.size(); k++)
+        if (bufB[k]) cudaFree(bufB[k]);
+    if (rc == MF_SUCCESS) rc = batch_build_items(B, best, run);
+    if (chosen) *chosen = best;
+    return rc;
 }

@@ -22,7 +22,7 @@ from . import _lib
 from ._lib import (MF_METHOD_BICGSTAB, MF_METHOD_CG, MF_PREC_FP64, MF_PREC_MIXED, MF_PREC_PARITY, MFError,
                    Options, Report, check)
 
-__all__ = ["Matrix", "Options", "Report", "MFError", "default_options", "read_matrix", "write_cbd",
+__all__ = ["Matrix", "Batch", "Options", "Report", "MFError", "default_options", "read_matrix", "write_cbd",
            "MF_PREC_FP64", "MF_PREC_MIXED", "MF_PREC_PARITY", "MF_METHOD_CG", "MF_METHOD_BICGSTAB"]
 
 _PREC = {"fp64": MF_PREC_FP64, "mixed": MF_PREC_MIXED, "parity": MF_PREC_PARITY}
@@ -233,6 +233,70 @@ class Matrix:
                                 _PREC[precision] if isinstance(precision, str) else precision,
                                 C.c_void_p(stream) if stream else None), "mf_spmv_noalloc")
         return y
+
+
+class Batch:
+    """Many independent systems solved in one persistent launch (mf_batch_*).
+
+        batch = Batch([A0, A1, ...], nrhs=[3, 1, ...])      # Matrix handles
+        batch.tune("mixed")                                 # right-hand sides per work item
+        Xs, reports = batch.solve([B0, B1, ...])            # CUDA tensors (nrhs_k, n_k)
+    """
+
+    def __init__(self, matrices, nrhs, stream=None):
+        L = _lib.load()
+        self._mats = list(matrices)         # the handles must outlive the batch
+        self.nrhs = [int(k) for k in nrhs]
+        h = C.c_void_p()
+        arr = (C.c_void_p * len(self._mats))(*[m._h for m in self._mats])
+        cnt = (C.c_int * len(self.nrhs))(*self.nrhs)
+        check(L.mf_batch_create(C.byref(h), len(self._mats), arr, cnt, C.c_void_p(stream) if stream else None),
+              "mf_batch_create")
+        self._h = h
+
+    def tune(self, precision="mixed", iters=20, stream=None) -> int:
+        cap = C.c_int()
+        check(_lib.load().mf_batch_tune(self._h, _PREC[precision] if isinstance(precision, str) else precision,
+                                        int(iters), C.byref(cap), C.c_void_p(stream) if stream else None),
+              "mf_batch_tune")
+        return cap.value
+
+    def solve(self, Bs, Xs=None, options: Options | None = None, use_graph=True, stream=None, **kw):
+        """Bs: CUDA float64 tensors of shape (nrhs_k, n_k).  Returns (Xs, reports)
+        with reports[k] the list of system k's per-column report dicts."""
+        import torch
+        L = _lib.load()
+        o = options if options is not None else default_options(**kw)
+        Bs = [b.contiguous() for b in Bs]
+        if Xs is None:
+            Xs = [torch.zeros_like(b) for b in Bs]
+        nb = len(Bs)
+        pb = (C.c_void_p * nb)(*[b.data_ptr() for b in Bs])
+        px = (C.c_void_p * nb)(*[x.data_ptr() for x in Xs])
+        reps = (Report * sum(self.nrhs))()
+        st = L.mf_batch_solve(self._h, pb, px, C.byref(o), reps, int(bool(use_graph)),
+                              C.c_void_p(stream) if stream else None)
+        flat = [r.as_dict() for r in reps]
+        out, k0 = [], 0
+        for k in self.nrhs:
+            out.append(flat[k0:k0 + k])
+            k0 += k
+        if st != _lib.MF_SUCCESS:
+            err = MFError(st, "mf_batch_solve")
+            err.report = out
+            raise err
+        return Xs, out
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().mf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def read_matrix(path: str):

@@ -201,6 +201,93 @@ def aniso2d_grf(N: int = 512, seed: int = 4, corr: float = 16.0, ratio: float = 
     return A, B, Xt, kap
 
 
+def _edge_stencil(shape, dirs, rng, sigma: float) -> CSR:
+    """SPD stencil matrix on a grid of `shape` (x fastest) from per-edge
+    coefficients: for every positive direction d in `dirs` and every cell p of
+    the grid padded by one ghost layer, one draw k = exp(sigma N(0,1)) for the
+    edge (p, p + d).  An edge between two cells adds k (e_i - e_j)(e_i - e_j)^T;
+    an edge from a cell to a ghost (Dirichlet boundary) adds k to the cell's
+    diagonal; ghost-ghost edges are dropped."""
+    dim = len(shape)
+    pad = tuple(s + 2 for s in shape[::-1])          # padded grid, slowest axis first
+    n = int(np.prod(shape))
+    grids = np.meshgrid(*[np.arange(-1, s + 1) for s in shape[::-1]], indexing="ij")
+    coords = [g.ravel() for g in grids[::-1]]       # x, y (, z) of every padded cell
+
+    def linear(c):
+        lin = np.zeros(c[0].size, np.int64)
+        stride = 1
+        for a in range(dim):
+            lin += np.clip(c[a], 0, shape[a] - 1) * stride
+            stride *= shape[a]
+        return lin
+
+    def inside_of(c):
+        ok = np.ones(c[0].size, bool)
+        for a in range(dim):
+            ok &= (c[a] >= 0) & (c[a] < shape[a])
+        return ok
+
+    inside, lin = inside_of(coords), linear(coords)
+    diag = np.zeros(n)
+    rows, cols, vals = [], [], []
+    for d in dirs:
+        k = np.exp(sigma * rng.standard_normal(pad)).ravel()
+        q = [coords[a] + d[a] for a in range(dim)]
+        inpad = np.ones(inside.size, bool)
+        for a in range(dim):
+            inpad &= (q[a] >= -1) & (q[a] <= shape[a])
+        qin, ql = inside_of(q), linear(q)
+        both = inside & qin & inpad
+        np.add.at(diag, lin[both], k[both])
+        np.add.at(diag, ql[both], k[both])
+        rows += [lin[both], ql[both]]
+        cols += [ql[both], lin[both]]
+        vals += [-k[both], -k[both]]
+        one = inpad & (inside ^ qin)                  # cell - ghost: boundary term of the inside cell
+        np.add.at(diag, np.where(inside, lin, ql)[one], k[one])
+    rows.append(np.arange(n))
+    cols.append(np.arange(n))
+    vals.append(diag)
+    import scipy.sparse as sp
+    S = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    S.sort_indices()
+    return CSR(n, S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data.astype(np.float64))
+
+
+def batch_systems(nsys: int = 512, seed: int = 3, side2d=(32, 512), side3d=(16, 64), rhs=(1, 16),
+                  sigma: float = 0.5):
+    """The batched workload: nsys independent SPD systems of uneven size.
+
+    default_rng(seed) first draws, for every system in order, its kind (2D
+    5-point or 3D 27-point, probability 1/2 each), its side (uniform integer in
+    side2d / side3d, inclusive) and its number of right-hand sides (uniform in
+    rhs, inclusive).  System k then uses its own stream
+    SeedSequence(seed).spawn(nsys)[k]: edge coefficients exp(sigma N(0,1))
+    (sigma the standard deviation) via _edge_stencil, then its right-hand sides
+    ~ N(0,1).  Returns a list of (kind, side, A, B) with B of shape (nrhs, n)."""
+    meta = np.random.default_rng(seed)
+    specs = []
+    for _ in range(nsys):
+        kind = "3d27" if meta.random() < 0.5 else "2d5"
+        lo, hi = side3d if kind == "3d27" else side2d
+        side = int(meta.integers(lo, hi + 1))
+        nr = int(meta.integers(rhs[0], rhs[1] + 1))
+        specs.append((kind, side, nr))
+    streams = [np.random.default_rng(s) for s in np.random.SeedSequence(seed).spawn(nsys)]
+    dirs2 = [(1, 0), (0, 1)]
+    dirs3 = [(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)
+             if (dz, dy, dx) > (0, 0, 0)]                                  # 13 of the 26 neighbours
+    out = []
+    for (kind, side, nr), rng in zip(specs, streams):
+        if kind == "2d5":
+            A = _edge_stencil((side, side), dirs2, rng, sigma)
+        else:
+            A = _edge_stencil((side, side, side), dirs3, rng, sigma)
+        out.append((kind, side, A, rng.standard_normal((nr, A.n))))
+    return out
+
+
 def random_csr(n: int, ncols: int, density: float, seed: int, shuffle_cols: bool = True,
                empty_rows: float = 0.0, dense_tile_rows: int = 0) -> CSR:
     """Random CSR with unsorted columns (when shuffle_cols), optional empty rows

@@ -1,0 +1,73 @@
+"""Batched solves (mf_batch_*): many uneven systems with 1 - 16 right-hand
+sides each in one persistent launch, against single-system solves.
+
+Tolerances: every column converges on its own FP64 true residual; columns
+agree with single-system solves to 1e-7 of max|x| at tol 1e-10 (same
+algorithm, block-level instead of grid-level reduction order)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def systems():
+    from millefeuille import matrices as M
+    return M.batch_systems(14, seed=3, side2d=(8, 48), side3d=(4, 12), rhs=(1, 16))
+
+
+def _relres(A, x, b):
+    return np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b)
+
+
+def _setup(mf, systems):
+    import torch
+    mats = [mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val) for _, _, A, _ in systems]
+    Bs = [torch.from_numpy(B).cuda() for _, _, _, B in systems]
+    return mats, Bs
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-8)])
+def test_batch_converges_and_matches_single_solves(mf, cuda, systems, precision, tol):
+    mats, Bs = _setup(mf, systems)
+    batch = mf.Batch(mats, [B.shape[0] for B in Bs])
+    Xs, reps = batch.solve(Bs, method="cg", precision=precision, tol=tol, use_graph=False)
+    for (kind, side, A, B), X, rk, G in zip(systems, Xs, reps, mats):
+        X = X.cpu().numpy()
+        assert len(rk) == B.shape[0]
+        for c in range(B.shape[0]):
+            assert rk[c]["converged"] and rk[c]["relres_true"] <= tol, (kind, side, c, rk[c])
+            assert _relres(A, X[c], B[c]) <= tol * 1.0001
+        if precision == "fp64":
+            xs, _ = G.solve(B[0], method="cg", precision="fp64", tol=tol)
+            np.testing.assert_allclose(X[0], xs, rtol=0, atol=1e-7 * np.abs(xs).max())
+
+
+def test_batch_graph_replay_and_tuning(mf, cuda, systems):
+    import torch
+    mats, Bs = _setup(mf, systems)
+    batch = mf.Batch(mats, [B.shape[0] for B in Bs])
+    X0, r0 = batch.solve(Bs, method="cg", precision="mixed", tol=1e-8, use_graph=False)
+    Xg, rg = batch.solve(Bs, method="cg", precision="mixed", tol=1e-8, use_graph=True)    # capture + run
+    Xs = [torch.full_like(b, 7.0) for b in Bs]
+    Xs, rr = batch.solve(Bs, Xs, method="cg", precision="mixed", tol=1e-8, use_graph=True)  # new X: recapture
+    Xs2, rr2 = batch.solve(Bs, Xs, method="cg", precision="mixed", tol=1e-8, use_graph=True)  # replay
+    for a, b, c, d in zip(X0, Xg, Xs, Xs2):
+        assert torch.equal(a, b) and torch.equal(a, c) and torch.equal(a, d)     # deterministic
+    assert [[x["iterations"] for x in s] for s in r0] == [[x["iterations"] for x in s] for s in rr2]
+    cap = batch.tune("mixed", iters=10)
+    assert cap in (2, 4, 8)
+    Xt, rt = batch.solve(Bs, method="cg", precision="mixed", tol=1e-8)
+    for (kind, side, A, B), X, rk in zip(systems, Xt, rt):
+        for c in range(B.shape[0]):
+            assert rk[c]["converged"] and _relres(A, X.cpu().numpy()[c], B[c]) <= 1.0001e-8
+
+
+def test_batch_rejects_bad_input(mf, cuda, systems):
+    mats, Bs = _setup(mf, systems[:2])
+    with pytest.raises(mf.MFError):
+        mf.Batch(mats, [0, 1])
+    batch = mf.Batch(mats, [B.shape[0] for B in Bs])
+    with pytest.raises(mf.MFError) as e:
+        batch.solve(Bs, method="bicgstab")
+    assert e.value.status == 5

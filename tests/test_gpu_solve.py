@@ -89,6 +89,25 @@ def test_gpu_cg_mixed_converges_fp64_verified(mf, oracle_mod, cuda, p3d):
     assert sum(rep["tile_uses"][1:]) > 0          # low-precision tiles were used
 
 
+def test_gpu_mixed_converges_past_the_fp32_floor(mf, cuda):
+    """A small well-conditioned 27-point system whose solve reaches the FP32
+    products' accuracy floor (~1e-7) early: the recursive residual collapses
+    below the true one, and the FP64 replacement must restart the direction
+    instead of scaling it by r_true.r_true / r_old.r_old (which broke down).
+    Single-column and multi-column kernels, CG; BiCGSTAB on the same system."""
+    from millefeuille import matrices as M
+    kind, side, A, B = M.batch_systems(14, seed=3, side2d=(8, 48), side3d=(4, 12), rhs=(1, 16))[0]
+    assert kind == "3d27" and A.n == 125
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    for method in ("cg", "bicgstab"):
+        x, rep = G.solve(B[0], method=method, precision="mixed", tol=1e-8)
+        assert rep["converged"] and rep["relres_true"] <= 1e-8 and rep["iterations"] < 500, (method, rep)
+        assert _relres(A, x, B[0]) <= 1.0001e-8
+    X, reps = G.solve_multi(B, method="cg", precision="mixed", tol=1e-8)
+    for k in range(B.shape[0]):
+        assert reps[k]["converged"] and reps[k]["iterations"] < 500 and _relres(A, X[k], B[k]) <= 1.0001e-8
+
+
 def test_gpu_cg_deterministic(mf, cuda, p3d):
     A, b, _ = p3d
     G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)

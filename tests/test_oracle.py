@@ -162,6 +162,22 @@ def test_generators_shapes():
     assert A.n == 4096 and pe == pytest.approx(10 * (2 * np.pi / 16) / 2, rel=0.03)  # max sin at cell centres < 1
 
 
+def test_batch_systems_generator():
+    """The batched workload: seeded kinds / sides / right-hand-side counts,
+    SPD 5-point and 27-point systems."""
+    from millefeuille import matrices as M
+    sy = M.batch_systems(8, seed=3, side2d=(6, 30), side3d=(3, 9), rhs=(1, 16))
+    sy2 = M.batch_systems(8, seed=3, side2d=(6, 30), side3d=(3, 9), rhs=(1, 16))
+    for (kind, side, A, B), (k2, s2, A2, B2) in zip(sy, sy2):
+        assert (kind, side) == (k2, s2) and np.array_equal(A.val, A2.val) and np.array_equal(B, B2)
+        n = side ** (2 if kind == "2d5" else 3)
+        assert A.n == n and B.shape[1] == n and 1 <= B.shape[0] <= 16
+        S = A.to_scipy()
+        assert abs(S - S.T).max() == 0
+        assert np.diff(A.rowptr).max() == (5 if kind == "2d5" else 27)
+        assert np.linalg.eigvalsh(S.toarray()).min() > 0
+
+
 def test_aniso2d_grf_generator():
     """The differentiable-solve workload: SPD 5-point system, GRF of unit
     variance, x-couplings ratio times the y-couplings, seeded."""
