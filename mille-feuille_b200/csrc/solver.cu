@@ -65,6 +65,7 @@ struct SolverParams {
     unsigned long long *counts;
     unsigned long long *phase_ns;   // [8] block-0 time per phase: spmv, vecB, vecC, barrier, replacement
     int method, max_iter, fixed_iters, replace_every, use_lossless;
+    int lossless_any;             // use_lossless and some tile is exact in INT8 / FP16
     double tol;
     float demote16, demote8;
     unsigned long long timeout_ns;
@@ -137,7 +138,7 @@ __device__ void block_partial(const SolverParams &P, Shared &sh, int kind, doubl
     if (wib == 0) {
         for (int k = 0; k < nv; k++) {
             const bool mx = (maxmask >> k) & 1u;
-            double a = (lane < kWarps) ? sh.wred[lane][k] : 0.0;
+            double a = (lane < kWarps) ? sh.wred[lane][k] : (mx ? -1.0e300 : 0.0);
 #pragma unroll
             for (int o = 16; o; o >>= 1) {
                 double b = __shfl_xor_sync(0xffffffffu, a, o);
@@ -156,7 +157,7 @@ __device__ void grid_collect(const SolverParams &P, Shared &sh, int kind, int nv
     if (wib == 0) {
         for (int k = 0; k < nv; k++) {
             const bool mx = (maxmask >> k) & 1u;
-            double a = 0.0;
+            double a = mx ? -1.0e300 : 0.0;
             for (int c = lane; c < (int)gridDim.x; c += 32) {
                 double b = P.red[((long long)kind * gridDim.x + c) * kRedWidth + k];
                 a = mx ? fmax(a, b) : a + b;
@@ -193,6 +194,7 @@ struct XVec {
     const signed char *lab;
     float invM;
     int force_pr;            // >= 0: every tile in this precision
+    int dyn;                 // mixed: 0 = no tile can leave FP32 in this SpMV (no precision lookups)
 };
 
 // Tile table of a slice, one tile per lane (lane i holds slot i).
@@ -212,7 +214,7 @@ __device__ __forceinline__ long long hdr_off(int4 h) { return (long long)h.w << 
 template <int MODE, bool F64>
 __device__ __forceinline__ float load_stat(const XVec &X, int tw, int i, int nt)
 {
-    if (F64 || MODE == MODE_FP64 || i >= nt || X.force_pr >= 0) return 0.0f;
+    if (F64 || MODE == MODE_FP64 || i >= nt || X.force_pr >= 0 || (MODE == MODE_MIXED && !X.dyn)) return 0.0f;
     const int jc = tw >> 8;
     if (MODE == MODE_MIXED) return X.mag[jc];
     return (float)X.lab[jc];
@@ -225,6 +227,7 @@ __device__ __forceinline__ int tile_prec(const SolverParams &P, int tw, float st
     if (F64 || MODE == MODE_FP64) return MF_P64;
     if (X.force_pr >= 0) return X.force_pr;
     if (MODE == MODE_PARITY) return parity_prec((int)st);
+    if (!X.dyn) return MF_P32;
     const unsigned cap = (unsigned)tw & 0xFFu;
     const float rel = st * X.invM;
     int pr = MF_P32;
@@ -522,12 +525,13 @@ __device__ __forceinline__ int8_t trunc_i8(double v)
 template <int MODE>
 __device__ __forceinline__ void publish_dir(int R, int row, bool valid, double vnew, double vold, float *v32,
                                             __half *v16, int8_t *v8, float *mag, signed char *lab, float &bmax,
-                                            unsigned hmask, bool labels)
+                                            unsigned hmask, bool labels, float *bmin = nullptr)
 {
     if (MODE != MODE_FP64 && valid) v32[row] = (float)vnew;
     if (MODE == MODE_MIXED) {
         float m = half_max(valid ? (float)fabs(vnew) : 0.0f, hmask);
         bmax = fmaxf(bmax, m);
+        if (bmin) *bmin = fminf(*bmin, m);
         if ((threadIdx.x & 15) == 0) mag[R] = m;
     } else if (MODE == MODE_PARITY) {
         if (valid) {
@@ -543,7 +547,7 @@ __device__ __forceinline__ void publish_dir(int R, int row, bool valid, double v
 }
 
 __device__ __forceinline__ XVec make_x(const double *x64, const float *x32, const __half *x16, const int8_t *x8,
-                                       const float *mag, const signed char *lab, float invM)
+                                       const float *mag, const signed char *lab, float invM, int dyn = 1)
 {
     XVec X;
     X.x64 = x64;
@@ -554,6 +558,7 @@ __device__ __forceinline__ XVec make_x(const double *x64, const float *x32, cons
     X.lab = lab;
     X.invM = invM;
     X.force_pr = -1;
+    X.dyn = dyn;
     return X;
 }
 
@@ -622,7 +627,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
 
     // ---- init: x = 0 (owned rows), r = b, p = r (rh = r) ----
     double pb = 0.0;
-    float bmax = 0.0f;
+    float bmax = 0.0f, bmin = 3.0e38f;
     for (int R = c.rbeg; R < c.rend; R++) {
         const int row = R * MF_BS + c.i;
         const bool valid = row < n;
@@ -634,13 +639,23 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             if (bicg) P.rh[row] = bv;
         }
         // parity mode: labels start all FP64 (cudaMemset(d_vis, 0), main-cg-mixed.cu:2828)
-        publish_dir<MODE>(R, row, valid, bv, 0.0, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, false);
+        publish_dir<MODE>(R, row, valid, bv, 0.0, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, false, &bmin);
         pb += bv * bv;
     }
-    block_partial(P, sh, 0, pb, (double)bmax, 0, 0, 2, 0x2u);
+    // the smallest segment magnitude (carried as -min) matters only to the mixed
+    // mode's SpMV; FP64 and parity reduce (sum, max) as before
+    constexpr int kNvSeg = (MODE == MODE_MIXED) ? 3 : 2;
+    block_partial(P, sh, 0, pb, (double)bmax, -(double)bmin, 0, kNvSeg, 0x6u);
     if (!grid_barrier(P, epoch, sh)) return;
-    double v[4];
-    grid_collect(P, sh, 0, 2, 0x2u, v);
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    grid_collect(P, sh, 0, kNvSeg, 0x6u, v);
+    // mixed: can any tile of the next SpMV leave FP32 at all?  Not when the
+    // smallest column segment is within demote_fp16 of the largest and no tile
+    // is exact in a narrower type: then the SpMV skips its precision lookups.
+    auto dyn_of = [&](double mx, double neg_mn) -> int {
+        return (P.lossless_any || mx <= 0.0 || -neg_mn <= (double)P.demote16 * mx) ? 1 : 0;
+    };
+    int dynA = (MODE == MODE_MIXED) ? dyn_of(v[1], v[2]) : 0;
             clk.lap(PH_BAR);
     const double bb = v[0];
     double rr = v[0], r1 = v[0];
@@ -666,7 +681,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             // ---- A: w = A r; p = r + beta p; q = w + beta q; p.q ----
             double ppq = 0.0;
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
-                                    make_x(P.r, P.r32, nullptr, nullptr, P.mag_r, nullptr, invM), cnt,
+                                    make_x(P.r, P.r32, nullptr, nullptr, P.mag_r, nullptr, invM, dynA), cnt,
                                     [&](int R, double y) {
                                         const int row = R * MF_BS + c.i;
                                         if (row < n) {
@@ -700,7 +715,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             if (!isfinite(alpha2)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B: x += alpha p; r -= alpha q; r.r; r's shadow ----
             double prr = 0.0;
-            float rmax = 0.0f;
+            float rmax = 0.0f, rmin = 3.0e38f;
             // kVB tile-rows per step: all loads first, so kVB round trips overlap
             for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
                 double xv[kVB], pv[kVB], rv[kVB], qv[kVB];
@@ -726,17 +741,18 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                         prr += rn * rn;
                     }
                     publish_dir<MODE>(R, row, valid, rn, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
-                                      c.hmask, false);
+                                      c.hmask, false, &rmin);
                 }
             }
             clk.lap(PH_VECB);
-            block_partial(P, sh, 2, prr, (double)rmax, 0, 0, 2, 0x2u);
+            block_partial(P, sh, 2, prr, (double)rmax, -(double)rmin, 0, kNvSeg, 0x6u);
             if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 2, 2, 0x2u, v);
+            grid_collect(P, sh, 2, kNvSeg, 0x6u, v);
             clk.lap(PH_BAR);
             double rr_new = v[0];
             const double rr_rec = rr_new;       // recursive r.r of this iteration
             invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
+            if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2]);
             k++;
             last_true = 0;
             const bool want_check = !P.fixed_iters && rr_new <= thr2;
@@ -746,6 +762,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 // ---- FP64 true residual r = b - A x (x is current), r's shadow ----
                 double prt = 0.0;
                 rmax = 0.0f;
+                rmin = 3.0e38f;
                 spmv_range<MODE, true>(P, c.sbeg, c.send, c.i, c.hmask, fp64_x(P.x), nullptr,
                                        [&](int R, double y) {
                                            const int row = R * MF_BS + c.i;
@@ -757,7 +774,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                                                prt += rv * rv;
                                            }
                                            publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr,
-                                                             P.mag_r, nullptr, rmax, c.hmask, false);
+                                                             P.mag_r, nullptr, rmax, c.hmask, false, &rmin);
                                        });
                 if (has_empty) {
                     for (int R = c.rbeg; R < c.rend; R++) {
@@ -770,16 +787,17 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                             prt += rv * rv;
                         }
                         publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
-                                          c.hmask, false);
+                                          c.hmask, false, &rmin);
                     }
                 }
                 clk.lap(PH_REPL);
-                block_partial(P, sh, 5, prt, (double)rmax, 0, 0, 2, 0x2u);
+                block_partial(P, sh, 5, prt, (double)rmax, -(double)rmin, 0, kNvSeg, 0x6u);
                 if (!grid_barrier(P, epoch, sh)) return;
-                grid_collect(P, sh, 5, 2, 0x2u, v);
+                grid_collect(P, sh, 5, kNvSeg, 0x6u, v);
                 clk.lap(PH_BAR);
                 rr_new = v[0];
                 invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
+                if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2]);
                 rr_true = rr_new;
                 repl++;
                 last_true = 1;
@@ -1205,10 +1223,10 @@ __device__ void grid_collect_m(const MultiParams &M, SharedM &sh, int kind, unsi
 template <int MODE, int NR, bool F64, typename Epi>
 __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se, int i, unsigned hmask,
                                            const double *X64, const float *X32, const float *mag, float invM,
-                                           Epi epi)
+                                           int dyn, Epi epi)
 {
     constexpr bool kMixed = (MODE == MODE_MIXED) && !F64;
-    XVec X = make_x(X64, X32, nullptr, nullptr, mag, nullptr, invM);
+    XVec X = make_x(X64, X32, nullptr, nullptr, mag, nullptr, invM, dyn);
     double acc[NR];
 #pragma unroll
     for (int k = 0; k < NR; k++) acc[k] = 0.0;
@@ -1227,7 +1245,9 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
         }
         const int xb = (tw >> 8) * MF_BS;
         int pr = MF_P64;
-        if (kMixed) {
+        if (kMixed && !dyn) {
+            pr = MF_P32;                 // no tile can leave FP32 in this SpMV: no lookups
+        } else if (kMixed) {
             const float st = (i < hdr_nt(h)) ? mag[tw >> 8] : 0.0f;
             pr = (i < hdr_nt(h)) ? tile_prec<MODE, false>(P, tw, st, X) : MF_P8;
 #pragma unroll
@@ -1413,6 +1433,12 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
     }
     __syncthreads();
     float invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
+    // mixed: some tile may leave FP32 only if the smallest segment is below
+    // demote_fp16 of the largest or lossless classes apply (see dyn in XVec)
+    auto dyn_of = [&](double mx, double neg_mn) -> int {
+        return (P.lossless_any || mx <= 0.0 || -neg_mn <= (double)P.demote16 * mx) ? 1 : 0;
+    };
+    int dyn = dyn_of(v[NR], v[NR + 1]);
     int k = 0, status = 0, repl = 0, last_true = 0;
     double rt[NR];
 #pragma unroll
@@ -1444,7 +1470,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
                 store_row<NR>(M.Q, row, q);
             }
         };
-        spmv_multi<MODE, NR, false>(P, c.sbeg, c.send, c.i, c.hmask, M.R, M.R32, M.mag, invM, upd_a);
+        spmv_multi<MODE, NR, false>(P, c.sbeg, c.send, c.i, c.hmask, M.R, M.R32, M.mag, invM, dyn, upd_a);
         if (has_empty) {
             double zw[NR];
 #pragma unroll
@@ -1499,6 +1525,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
         prr[NR + 1] = -st.mn;
         if (!sy.template reduce<NR + 2>(2, prr, mm2, v)) return;
         invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
+        dyn = dyn_of(v[NR], v[NR + 1]);
         k++;
         last_true = 0;
         bool want_repl = P.replace_every > 0 && (k % P.replace_every) == 0;
@@ -1531,7 +1558,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
                 }
                 publish_multi<MODE, NR>(M, R, row, valid, r, st, c.hmask);
             };
-            spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, upd_r);
+            spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, 1, upd_r);
             if (has_empty) {
                 double zy[NR];
 #pragma unroll
@@ -1543,6 +1570,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
             prt[NR + 1] = -st.mn;
             if (!sy.template reduce<NR + 2>(5, prt, mm2, v)) return;
             invM = v[NR] > 0.0 ? (float)(1.0 / v[NR]) : 0.0f;
+            dyn = dyn_of(v[NR], v[NR + 1]);
             repl++;
             last_true = 1;
 #pragma unroll
@@ -1580,7 +1608,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
                 for (int j = 0; j < NR; j++) prt[j] += (b[j] - y[j]) * (b[j] - y[j]);
             }
         };
-        spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, acc_r);
+        spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, 1, acc_r);
         if (has_empty) {
             double zy[NR];
 #pragma unroll
@@ -1763,6 +1791,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
         P.fixed_iters = B.fixed_iters;
         P.replace_every = B.replace_every;
         P.use_lossless = B.use_lossless;
+        P.lossless_any = B.use_lossless;     // conservative: the batch does not scan its tiles
         P.tol = B.tol;
         P.demote16 = B.demote16;
         P.demote8 = B.demote8;
@@ -1801,6 +1830,7 @@ struct Workspace {
     int *hw_begin;
     int nhw;
     cudaEvent_t e0, e1;
+    int any_exact;         // some tile is exact in INT8 or FP16 (lossless classes can apply)
     // several right-hand sides (k_solve_multi): interleaved vectors for NR columns
     int m_nr, m_G;
     double *m_vec;         // B | X | R | P | Q, each vec_len * NR
@@ -1821,6 +1851,15 @@ int dal(T **p, long long count)
         int _rc = (expr);                   \
         if (_rc != MF_SUCCESS) return _rc;  \
     } while (0)
+
+__global__ void k_any_exact(const unsigned char *caps, int n, int *flag)
+{
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        if (caps[t] & (MF_CAP_EXACT_I8 | MF_CAP_EXACT_F16)) {
+            atomicOr(flag, 1);
+            return;
+        }
+}
 
 const void *solve_kernel(int mode, int lb)
 {
@@ -1896,6 +1935,14 @@ int ws_get(mf_matrix_s *A, int blocks_per_sm, Workspace **out, cudaStream_t s)
     MF_TRY(dal(&w->bar, 1)); MF_TRY(dal(&w->err, 1)); MF_TRY(dal(&w->out, 16));
     MF_TRY(dal(&w->counts, 16));
     MF_TRY(dal(&w->phase_ns, 8));
+    {
+        int *flag = (int *)w->counts;       // scratch before the first solve zeroes it
+        MF_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), s));
+        if (A->tilenum > 0) k_any_exact<<<256, 256, 0, s>>>(A->d_tile_caps, A->tilenum, flag);
+        MF_CUDA_TRY(cudaGetLastError());
+        MF_CUDA_TRY(cudaMemcpyAsync(&w->any_exact, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MF_CUDA_TRY(cudaStreamSynchronize(s));
+    }
     w->nhw = G * kWarps * 2;
     MF_TRY(dal(&w->hw_begin, w->nhw + 1));
     MF_CUDA_TRY(cudaEventCreate(&w->e0));
@@ -2048,6 +2095,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     P.fixed_iters = opt->fixed_iters;
     P.replace_every = opt->replace_every;
     P.use_lossless = opt->use_lossless;
+    P.lossless_any = (opt->use_lossless && w->any_exact) ? 1 : 0;
     P.tol = opt->tol;
     P.demote16 = (float)opt->demote_fp16;
     P.demote8 = (float)opt->demote_int8;
@@ -2324,6 +2372,7 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
     P.fixed_iters = opt->fixed_iters;
     P.replace_every = opt->replace_every;
     P.use_lossless = opt->use_lossless;
+    P.lossless_any = (opt->use_lossless && w->any_exact) ? 1 : 0;
     P.tol = opt->tol;
     P.demote16 = (float)opt->demote_fp16;
     P.demote8 = (float)opt->demote_int8;

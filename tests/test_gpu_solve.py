@@ -89,6 +89,23 @@ def test_gpu_cg_mixed_converges_fp64_verified(mf, oracle_mod, cuda, p3d):
     assert sum(rep["tile_uses"][1:]) > 0          # low-precision tiles were used
 
 
+def test_gpu_mixed_demotes_small_segments_and_converges(mf, cuda, p3d):
+    """A right-hand side confined to a few planes: most column segments of the
+    SpMV operand are tiny or zero next to the largest, so their tiles run in
+    FP16 / INT8; the solve still converges on the FP64 true residual.  A
+    uniform right-hand side of the same system keeps every tile in FP32."""
+    A, _, _ = p3d
+    b = np.zeros(A.n)
+    b[:3 * 32 * 32] = np.random.default_rng(3).standard_normal(3 * 32 * 32)
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x, rep = G.solve(b, method="cg", precision="mixed", tol=1e-8)
+    assert rep["converged"] and _relres(A, x, b) <= 1.0001e-8
+    assert rep["tile_uses"][2] + rep["tile_uses"][3] > 0, rep["tile_uses"]
+    X, reps = G.solve_multi(np.stack([b, b[::-1].copy()]), method="cg", precision="mixed", tol=1e-8)
+    for k in range(2):
+        assert reps[k]["converged"] and _relres(A, X[k], [b, b[::-1]][k]) <= 1.0001e-8
+
+
 def test_gpu_mixed_converges_past_the_fp32_floor(mf, cuda):
     """A small well-conditioned 27-point system whose solve reaches the FP32
     products' accuracy floor (~1e-7) early: the recursive residual collapses
