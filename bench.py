@@ -153,8 +153,10 @@ def run_ours(args, rank, world, local_rank):
     def timed(opt, steps, host=False):
         reps = []
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        hb = b.copy()
-        hx = np.zeros_like(hb)
+        # end-to-end inputs and outputs live in pinned host memory (page-locked,
+        # so the copies inside the solve call are DMA transfers)
+        hb = torch.from_numpy(b).pin_memory().numpy()
+        hx = torch.zeros(b.size, dtype=torch.float64).pin_memory().numpy()
         sync_all()
         ev0.record(stream)
         for _ in range(steps):
@@ -246,44 +248,66 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_adjoint:
         out["config"]["fwd_adjoint"] = fwd_adjoint(dev, args.adjoint_rhs)
     if not args.no_batch:
-        out["config"]["batch"] = batch_line(dev, args.batch_systems)
+        out["config"]["batch"] = batch_line(dev, args.batch_systems, rank, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(A, b, rep64["iterations"], budget_s=args.cpu_budget)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
 
-def batch_line(dev, nsys):
+def batch_line(dev, nsys, rank=0, world=1):
     """Batched uneven solves: nsys independent SPD systems (2D 5-point sides
     U{32..512} / 3D 27-point sides U{16..64}, coefficients exp(0.5 N(0,1)),
-    1-16 right-hand sides each, seed 3) in one persistent launch, mixed CG to
-    1e-8, right-hand sides per work item tuned, the enqueue sequence replayed
-    from a CUDA graph.  One untimed solve (capture), then one timed replay."""
+    1-16 right-hand sides each, seed 3) in one persistent launch per GPU, mixed
+    CG to 1e-8, right-hand sides per work item tuned, the enqueue sequence
+    replayed from a CUDA graph.  With N ranks every rank generates and solves
+    only the systems mf_batch_partition gives it (no collective on the data
+    path); the batch time is the slowest rank's, the reports are gathered on
+    rank 0.  One untimed solve (capture), then one timed replay."""
     import torch
     import millefeuille as mf
     from millefeuille import matrices as M
+    from millefeuille import shard
+    specs = M.batch_specs(nsys, seed=3)
+    part, loads = shard.partition([sp[3] for sp in specs], [sp[4] for sp in specs], [sp[2] for sp in specs], world)
+    own = shard.owned(part, rank)
     t0 = time.perf_counter()
-    systems = M.batch_systems(nsys, seed=3)
+    systems = M.batch_systems(nsys, seed=3, only=own)
     gen_s = time.perf_counter() - t0
-    mats = [mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val) for _, _, A, _ in systems]
-    Bs = [torch.from_numpy(B).to(dev) for _, _, _, B in systems]
-    batch = mf.Batch(mats, [B.shape[0] for B in Bs])
-    cap = batch.tune("mixed", iters=20)
-    Xs = [torch.zeros_like(b) for b in Bs]
-    o = mf.default_options(precision="mixed", tol=TOL, max_iter=20000)
-    batch.solve(Bs, Xs, options=o, use_graph=True)
-    torch.cuda.synchronize(dev)
-    _, reps = batch.solve(Bs, Xs, options=o, use_graph=True)
+    reps, ms, cap = [], 0.0, 0
+    if own:
+        mats = [mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val) for _, _, A, _ in systems]
+        Bs = [torch.from_numpy(B).to(dev) for _, _, _, B in systems]
+        batch = mf.Batch(mats, [B.shape[0] for B in Bs])
+        cap = batch.tune("mixed", iters=20)
+        Xs = [torch.zeros_like(b) for b in Bs]
+        o = mf.default_options(precision="mixed", tol=TOL, max_iter=20000)
+        batch.solve(Bs, Xs, options=o, use_graph=True)
+        torch.cuda.synchronize(dev)
+        _, reps = batch.solve(Bs, Xs, options=o, use_graph=True)
+        ms = reps[0][0]["time_ms"]
+        batch.close()
+    if world > 1:
+        ms = shard.max_over_ranks(ms, device=dev)
+        gen_s = shard.max_over_ranks(gen_s, device=dev)
+        reps = shard.gather_reports(own, reps, nsys)
+        if rank != 0:
+            return None
     flat = [r for s_ in reps for r in s_]
     its = [r["iterations"] for r in flat]
-    return {"workload": f"{nsys} systems ({sum(k == '2d5' for k, *_ in systems)} 2D 5-point, "
-                        f"{sum(k == '3d27' for k, *_ in systems)} 3D 27-point), seed 3, mixed CG tol 1e-8",
-            "nnz_total": int(sum(A.nnz for _, _, A, _ in systems)), "rhs_total": len(flat),
-            "unknowns_x_rhs": int(sum(A.n * B.shape[0] for _, _, A, B in systems)),
-            "solve_ms": round(flat[0]["time_ms"], 3), "rhs_per_item": cap,
-            "converged": int(sum(r["converged"] for r in flat)), "relres_true_max": max(r["relres_true"] for r in flat),
-            "iterations_mean": round(sum(its) / len(its), 1), "iterations_max": max(its),
-            "grid": [flat[0]["grid_blocks"], flat[0]["threads_per_block"]], "host_generation_s": round(gen_s, 1)}
+    out = {"workload": f"{nsys} systems ({sum(sp[0] == '2d5' for sp in specs)} 2D 5-point, "
+                       f"{sum(sp[0] == '3d27' for sp in specs)} 3D 27-point), seed 3, mixed CG tol 1e-8",
+           "nnz_total": int(sum(sp[4] for sp in specs)), "rhs_total": len(flat),
+           "unknowns_x_rhs": int(sum(sp[2] * sp[3] for sp in specs)),
+           "solve_ms": round(ms, 3), "rhs_per_item": cap,
+           "converged": int(sum(r["converged"] for r in flat)), "relres_true_max": max(r["relres_true"] for r in flat),
+           "iterations_mean": round(sum(its) / len(its), 1), "iterations_max": max(its),
+           "grid": [flat[0]["grid_blocks"], flat[0]["threads_per_block"]], "host_generation_s": round(gen_s, 1)}
+    if world > 1:
+        out["split"] = {"gpus": world, "systems_per_gpu": [part.count(q) for q in range(world)],
+                        "estimated_load_imbalance": round(max(loads) / (sum(loads) / world), 3),
+                        "rhs_per_item_rank0": cap}
+    return out
 
 
 def fwd_adjoint(dev, nrhs):

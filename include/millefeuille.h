@@ -236,6 +236,20 @@ int mf_batch_solve(mf_batch b, const double *const *B, double *const *X, const m
                    mf_report *reports, int use_graph, void *stream);
 int mf_batch_destroy(mf_batch b);
 
+/*
+ * Split of a batch's systems over nparts GPUs (one process per GPU, each with
+ * its own mf_batch of the systems it owns; no collective on the data path).
+ * Greedy longest-processing-time over whole systems, by decreasing estimated
+ * cost -- the sum over the system's work items of groups of <= cap columns
+ * (cap 1..8; <= 0 means 8) of nnz * (1 + 0.35 (width - 1)) * sqrt(n), the cost
+ * the work queue orders by -- each to the least-loaded part so far; ties go to
+ * the lower index.  part[k] (nsys ints) gets system k's part; load (nullable,
+ * nparts doubles) each part's total cost.  Host only, deterministic: every rank
+ * computes the same split.  No counterpart in the reference.
+ */
+int mf_batch_partition(int nsys, const int *n, const long long *nnz, const int *nrhs, int cap, int nparts,
+                       int *part, double *load);
+
 /* y = A x with the tile kernel.  precision: MF_PREC_FP64 or MF_PREC_MIXED
  * (MIXED here means every tile in FP32).  elapsed_ms (nullable) gets the kernel time. */
 int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs,

@@ -365,6 +365,39 @@ extern "C" int mf_batch_destroy(mf_batch b)
     return MF_SUCCESS;
 }
 
+// Greedy longest-processing-time split of whole systems over nparts GPUs: the
+// systems by decreasing cost (ties: lower index first), each to the part with
+// the least load so far (ties: lower part).  A system's cost is the sum over its
+// work items (groups of <= cap columns) of the queue's item cost.  Host only;
+// every rank computes the same split from the same inputs.
+extern "C" int mf_batch_partition(int nsys, const int *n, const long long *nnz, const int *nrhs, int cap,
+                                  int nparts, int *part, double *load)
+{
+    if (nsys < 0 || nparts < 1 || (nsys > 0 && (!n || !nnz || !nrhs || !part))) return MF_ERR_INVALID;
+    if (cap <= 0) cap = 8;
+    if (cap > 8) return MF_ERR_INVALID;
+    std::vector<double> cost(nsys, 0.0);
+    for (int k = 0; k < nsys; k++) {
+        if (n[k] < 1 || nnz[k] < 0 || nrhs[k] < 1) return MF_ERR_INVALID;
+        for (int c0 = 0; c0 < nrhs[k]; c0 += cap)
+            cost[k] += mf_batch_item_cost(nnz[k], n[k], mf_batch_width(std::min(cap, nrhs[k] - c0)));
+    }
+    std::vector<int> order(nsys);
+    for (int k = 0; k < nsys; k++) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<double> ld(nparts, 0.0);
+    for (int k : order) {
+        int best = 0;
+        for (int q = 1; q < nparts; q++)
+            if (ld[q] < ld[best]) best = q;
+        part[k] = best;
+        ld[best] += cost[k];
+    }
+    if (load)
+        for (int q = 0; q < nparts; q++) load[q] = ld[q];
+    return MF_SUCCESS;
+}
+
 extern "C" int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs, void *stream,
                        double *elapsed_ms)
 {

@@ -17,6 +17,7 @@
 //    entries of row i appear tile by tile (slot order), within a tile in the
 //    reference payload order.  Per tile: int8 scale and capability flags.
 #pragma once
+#include <cmath>
 
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
@@ -115,6 +116,15 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
                   mf_report *rep, cudaStream_t s);
 int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X, const mf_options *opt,
                         mf_report *reps, cudaStream_t s);
+// Batched work items: interleave width of a group of g columns, and the
+// estimated work of an item (entries x widened columns x iterations, the CG
+// iteration count of these systems taken as ~ sqrt(n)).  The device queue's
+// order and the split across GPUs (mf_batch_partition) both use it.
+inline int mf_batch_width(int g) { return g >= 5 ? 8 : g >= 3 ? 4 : g == 2 ? 2 : 1; }
+inline double mf_batch_item_cost(long long nnz, int n, int width)
+{
+    return (double)nnz * (1.0 + 0.35 * (double)(width - 1)) * std::sqrt((double)(n > 1 ? n : 1));
+}
 int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems, const int *nrhs, cudaStream_t s);
 int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *Xd, const mf_options *opt,
                         mf_report *reps, int use_graph, cudaStream_t s);

@@ -2483,7 +2483,7 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
             B.it_sys.push_back(k);
             B.it_col0.push_back(c0);
             B.it_ncol.push_back(g);
-            B.it_nr.push_back(g >= 5 ? 8 : g >= 3 ? 4 : g == 2 ? 2 : 1);
+            B.it_nr.push_back(mf_batch_width(g));
         }
     B.nitems = (int)B.it_sys.size();
     // per item: B | X | R | P | Q (doubles), R32 (floats), segment magnitudes, report words
@@ -2522,8 +2522,7 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
         it.M.red = nullptr;
         it.M.out = (double *)(B.d_pool + B.out_off[t]);
         it.M.nr = B.it_ncol[t];
-        // estimated work: entries x (widened) columns x iterations (~ sqrt(n) for these systems)
-        cost[t] = (double)A->nnz * (1.0 + 0.35 * (double)(nr - 1)) * std::sqrt((double)std::max(1, A->n_rows));
+        cost[t] = mf_batch_item_cost(A->nnz, A->n_rows, (int)nr);
     }
     std::vector<int> order(B.nitems);
     for (int t = 0; t < B.nitems; t++) order[t] = t;

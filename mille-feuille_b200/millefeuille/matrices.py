@@ -255,8 +255,29 @@ def _edge_stencil(shape, dirs, rng, sigma: float) -> CSR:
     return CSR(n, S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data.astype(np.float64))
 
 
+def batch_specs(nsys: int = 512, seed: int = 3, side2d=(32, 512), side3d=(16, 64), rhs=(1, 16)):
+    """The batched workload's system list without building it: for every system
+    (kind, side, nrhs, n, nnz), drawn exactly as batch_systems draws them.  A 2D
+    5-point system has n = side^2 and nnz = 5 n - 4 side; a 3D 27-point system
+    has n = side^3 and nnz = (3 side - 2)^3 (each axis couples a cell to itself
+    and its two neighbours: 3 side - 2 pairs per axis)."""
+    meta = np.random.default_rng(seed)
+    out = []
+    for _ in range(nsys):
+        kind = "3d27" if meta.random() < 0.5 else "2d5"
+        lo, hi = side3d if kind == "3d27" else side2d
+        side = int(meta.integers(lo, hi + 1))
+        nr = int(meta.integers(rhs[0], rhs[1] + 1))
+        if kind == "2d5":
+            n, nnz = side * side, 5 * side * side - 4 * side
+        else:
+            n, nnz = side ** 3, (3 * side - 2) ** 3
+        out.append((kind, side, nr, n, nnz))
+    return out
+
+
 def batch_systems(nsys: int = 512, seed: int = 3, side2d=(32, 512), side3d=(16, 64), rhs=(1, 16),
-                  sigma: float = 0.5):
+                  sigma: float = 0.5, only=None):
     """The batched workload: nsys independent SPD systems of uneven size.
 
     default_rng(seed) first draws, for every system in order, its kind (2D
@@ -265,21 +286,18 @@ def batch_systems(nsys: int = 512, seed: int = 3, side2d=(32, 512), side3d=(16, 
     rhs, inclusive).  System k then uses its own stream
     SeedSequence(seed).spawn(nsys)[k]: edge coefficients exp(sigma N(0,1))
     (sigma the standard deviation) via _edge_stencil, then its right-hand sides
-    ~ N(0,1).  Returns a list of (kind, side, A, B) with B of shape (nrhs, n)."""
-    meta = np.random.default_rng(seed)
-    specs = []
-    for _ in range(nsys):
-        kind = "3d27" if meta.random() < 0.5 else "2d5"
-        lo, hi = side3d if kind == "3d27" else side2d
-        side = int(meta.integers(lo, hi + 1))
-        nr = int(meta.integers(rhs[0], rhs[1] + 1))
-        specs.append((kind, side, nr))
-    streams = [np.random.default_rng(s) for s in np.random.SeedSequence(seed).spawn(nsys)]
+    ~ N(0,1).  Returns a list of (kind, side, A, B) with B of shape (nrhs, n);
+    with `only` (system indices) just those systems, in that order, identical
+    to the same entries of the full list."""
+    specs = batch_specs(nsys, seed, side2d, side3d, rhs)
+    seeds = np.random.SeedSequence(seed).spawn(nsys)
     dirs2 = [(1, 0), (0, 1)]
     dirs3 = [(dx, dy, dz) for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)
              if (dz, dy, dx) > (0, 0, 0)]                                  # 13 of the 26 neighbours
     out = []
-    for (kind, side, nr), rng in zip(specs, streams):
+    for k in (range(nsys) if only is None else only):
+        kind, side, nr, _, _ = specs[k]
+        rng = np.random.default_rng(seeds[k])
         if kind == "2d5":
             A = _edge_stencil((side, side), dirs2, rng, sigma)
         else:

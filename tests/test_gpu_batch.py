@@ -71,3 +71,24 @@ def test_batch_rejects_bad_input(mf, cuda, systems):
     with pytest.raises(mf.MFError) as e:
         batch.solve(Bs, method="bicgstab")
     assert e.value.status == 5
+
+
+def test_batch_split_over_parts_matches_one_batch(mf, cuda, systems):
+    """The multi-GPU split run part by part on one GPU (each part its own
+    mf_batch, as each rank would): every system's solution is bitwise the one
+    the single batch gives (an item's arithmetic does not depend on the block,
+    the launch or the other items)."""
+    import torch
+    from millefeuille import shard
+    mats, Bs = _setup(mf, systems)
+    nr = [B.shape[0] for B in Bs]
+    X1, r1 = mf.Batch(mats, nr).solve(Bs, method="cg", precision="mixed", tol=1e-8, use_graph=False)
+    part, _ = shard.partition([A.n for _, _, A, _ in systems], [A.nnz for _, _, A, _ in systems], nr, 3)
+    for q in range(3):
+        own = shard.owned(part, q)
+        assert own
+        Xq, rq = mf.Batch([mats[k] for k in own], [nr[k] for k in own]).solve(
+            [Bs[k] for k in own], method="cg", precision="mixed", tol=1e-8, use_graph=False)
+        for k, X, rk in zip(own, Xq, rq):
+            assert torch.equal(X, X1[k])
+            assert [x["iterations"] for x in rk] == [x["iterations"] for x in r1[k]]
