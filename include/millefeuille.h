@@ -223,7 +223,10 @@ int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_o
  *                  (nullable) gets the choice.
  * mf_batch_solve   B[k] / X[k]: DEVICE arrays of nrhs[k] x n_k doubles (one
  *                  vector after another).  reports (nullable): sum(nrhs)
- *                  records, system by system; time_ms is the whole batch's.
+ *                  records, system by system; time_ms is the whole batch's;
+ *                  phase_ms[0] / [1]: the column's work item's start and end
+ *                  in ms after the launch's first item start, phase_ms[2]: the
+ *                  blocks that solved it.
  *                  use_graph != 0: the enqueue sequence (interleave, queue
  *                  reset, launch, de-interleave) is captured into a CUDA graph
  *                  on first use and replayed while the pointers and options stay
@@ -241,7 +244,7 @@ int mf_batch_destroy(mf_batch b);
  * its own mf_batch of the systems it owns; no collective on the data path).
  * Greedy longest-processing-time over whole systems, by decreasing estimated
  * cost -- the sum over the system's work items of groups of <= cap columns
- * (cap 1..8; <= 0 means 8) of nnz * (1 + 0.35 (width - 1)) * sqrt(n), the cost
+ * (cap 1..8; <= 0 means 8) of (n + nnz / 64) * (1 + 0.35 (width - 1)) * n^0.4, the cost
  * the work queue orders by -- each to the least-loaded part so far; ties go to
  * the lower index.  part[k] (nsys ints) gets system k's part; load (nullable,
  * nparts doubles) each part's total cost.  Host only, deterministic: every rank

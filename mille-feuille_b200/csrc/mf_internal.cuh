@@ -117,13 +117,19 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
 int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X, const mf_options *opt,
                         mf_report *reps, cudaStream_t s);
 // Batched work items: interleave width of a group of g columns, and the
-// estimated work of an item (entries x widened columns x iterations, the CG
-// iteration count of these systems taken as ~ sqrt(n)).  The device queue's
-// order and the split across GPUs (mf_batch_partition) both use it.
+// estimated time of an item on one block: iterations x per-iteration work.
+// Measured on one B200 (512-thread blocks, mixed CG, 8 columns), the
+// per-iteration time of one block is set by the rows (the vector phases and
+// the per-row gathers), not by the entries: a 5-point and a 27-point system of
+// ~250,000 rows took the same time per row within 10 %; entries count as 1/64
+// of a row.  Iterations are taken as n^0.4 (CG on these diffusion systems
+// needs ~ side iterations: n^0.5 in 2D, n^0.33 in 3D).  The device queue's
+// order, the team sizes and the split across GPUs (mf_batch_partition) all use it.
 inline int mf_batch_width(int g) { return g >= 5 ? 8 : g >= 3 ? 4 : g == 2 ? 2 : 1; }
 inline double mf_batch_item_cost(long long nnz, int n, int width)
 {
-    return (double)nnz * (1.0 + 0.35 * (double)(width - 1)) * std::sqrt((double)(n > 1 ? n : 1));
+    const double rows = (double)(n > 1 ? n : 1);
+    return (rows + (double)nnz / 64.0) * (1.0 + 0.35 * (double)(width - 1)) * std::pow(rows, 0.4);
 }
 int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems, const int *nrhs, cudaStream_t s);
 int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *Xd, const mf_options *opt,

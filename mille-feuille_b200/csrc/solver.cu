@@ -1162,9 +1162,11 @@ struct MultiParams {
     int nr;                   // columns in use
 };
 
-// Block partial of NV values (maxmask bit k: max instead of sum) into red[kind][block][*].
+// Block partial of NV values (maxmask bit k: max instead of sum) into
+// red[kind][bidx][*] of an nblk-block group (the grid, or a batched item's team).
 template <int NV>
-__device__ void block_partial_m(const MultiParams &M, SharedM &sh, int kind, const double (&v)[NV], unsigned maxmask)
+__device__ void block_partial_m(const MultiParams &M, SharedM &sh, int kind, const double (&v)[NV], unsigned maxmask,
+                                int nblk, int bidx)
 {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 #pragma unroll
@@ -1188,20 +1190,22 @@ __device__ void block_partial_m(const MultiParams &M, SharedM &sh, int kind, con
             const double b = __shfl_xor_sync(0xffffffffu, a, o);
             a = mx ? fmax(a, b) : a + b;
         }
-        if (lane == 0) M.red[((long long)kind * gridDim.x + blockIdx.x) * kRedWidthM + wib] = a;
+        if (lane == 0) M.red[((long long)kind * nblk + bidx) * kRedWidthM + wib] = a;
     }
 }
 
-// After the sync: every block sums the block partials of `kind` in the same order.
+// After the sync: every block of the group sums the nblk partials of `kind` in
+// the same order.
 template <int NV>
-__device__ void grid_collect_m(const MultiParams &M, SharedM &sh, int kind, unsigned maxmask, double (&out)[NV])
+__device__ void grid_collect_m(const MultiParams &M, SharedM &sh, int kind, unsigned maxmask, double (&out)[NV],
+                               int nblk)
 {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     if (wib < NV) {
         const bool mx = (maxmask >> wib) & 1u;
         double a = mx ? -1.0e300 : 0.0;
-        for (int c = lane; c < (int)gridDim.x; c += 32) {
-            const double b = M.red[((long long)kind * gridDim.x + c) * kRedWidthM + wib];
+        for (int c = lane; c < nblk; c += 32) {
+            const double b = M.red[((long long)kind * nblk + c) * kRedWidthM + wib];
             a = mx ? fmax(a, b) : a + b;
         }
 #pragma unroll
@@ -1644,9 +1648,9 @@ struct GridSync {
     template <int NV>
     __device__ bool reduce(int kind, const double (&v)[NV], unsigned maxmask, double (&out)[NV])
     {
-        block_partial_m<NV>(M, sh, kind, v, maxmask);
+        block_partial_m<NV>(M, sh, kind, v, maxmask, (int)gridDim.x, (int)blockIdx.x);
         if (!grid_barrier(P, epoch, sh)) return false;
-        grid_collect_m<NV>(M, sh, kind, maxmask, out);
+        grid_collect_m<NV>(M, sh, kind, maxmask, out, (int)gridDim.x);
         return true;
     }
     __device__ bool writer() const { return blockIdx.x == 0 && threadIdx.x == 0; }
@@ -1662,12 +1666,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
 }
 
 // ------------------------------------------------------------ batched systems
-// Many independent systems in one persistent launch.  A device work queue holds
-// (system, up to 8 of its right-hand sides) items, largest estimated cost first;
-// every block takes the next item, solves it alone with the CG body above --
-// block-level syncs instead of grid syncs, so the launch needs no co-residency
-// and can be captured in a CUDA graph -- and then takes the next one.
+// Many independent systems in one persistent launch of one 512-thread block
+// per SM.  Work items are (system, up to 8 of its right-hand sides).
+//  * Team items: an item whose estimated cost exceeds a fair share of the
+//    launch (total cost / blocks) is solved by a team of k blocks, sized by its
+//    cost; the host list-schedules team items onto blocks (the k blocks that
+//    are free first) and gives every block its ordered list.  Team members
+//    synchronise through a counter of their own (bounded waits) and reduce in
+//    a fixed order over the k block partials.
+//  * Queue items: everything else sits in a device work queue, largest
+//    estimated cost first; a block that has finished its list takes the next
+//    queue item and solves it alone with block-level syncs.
+// The launch is cooperative, so every block is resident and a team never waits
+// on a block that cannot run; the lists are sorted by the same global order
+// (scheduled start, then item), so no two teams wait on each other.
 constexpr int kHalvesPerBlock = kWarps * 2;
+constexpr int kMinTeamRows = 64;  // tile-rows per team block at least (2 per half-warp)
+// Team size = round(kTeamGrain x cost / fair share): a team's members finish an
+// item in about 1 / kTeamGrain of a fair share, so no single item sets the
+// launch's end.  A team costs a few microseconds per sync, small against the
+// milliseconds a large item's iteration takes on one block.
+// Measured on the 512-system batch: grain 1, 2, 4 -> 20.2, 18.7, 17.8 s.
+constexpr double kTeamGrain = 4.0;
 
 struct BatchItem {
     const int *seg_ptr;
@@ -1681,15 +1701,22 @@ struct BatchItem {
     const int8_t *v8;
     const float *i8_scale;
     const long long *row_cost;    // tile-row cost prefix [tilem + 1]
-    MultiParams M;                // the item's interleaved vectors and report words (M.nr columns used)
+    MultiParams M;                // the item's interleaved vectors and report words (M.nr columns used);
+                                  // team items: M.red holds the team's partials [kinds][team][kRedWidthM]
+    unsigned *ctr;                // team items: the team's barrier counter (zeroed before the launch)
     int n, tilem, nr;             // nr: interleave width (1, 2, 4 or 8)
+    int team;                     // blocks solving the item (1: queue item)
 };
 
 struct BatchParams {
     const BatchItem *items;
-    const int *order;             // item indices, largest estimated cost first
-    int n_items;
+    const int *order;             // queue items, largest estimated cost first
+    int n_items;                  // queue items
     unsigned *head;               // next position in `order` (zeroed before the launch)
+    const int *bptr;              // [grid + 1] each block's list of team entries
+    const int2 *blist;            // (item, rank in its team)
+    int *err;                     // first error of a team wait (zeroed before the launch)
+    unsigned long long timeout_ns, arrive_timeout_ns;
     int max_iter, fixed_iters, replace_every, use_lossless;
     double tol;
     float demote16, demote8;
@@ -1733,8 +1760,76 @@ struct BlockSync {
     __device__ bool writer() const { return threadIdx.x == 0; }
 };
 
-// The half-warps of one block split a system's tile-rows by the cost prefix.
-__device__ __forceinline__ Ctx block_ctx(const BatchItem &it)
+// Barrier of the k blocks of one team: a monotone counter with the pattern of
+// grid_barrier (fence, relaxed add, relaxed polls, one acquire fence), bounded
+// by `limit_ns`; a timeout, or an error set elsewhere, returns false and the
+// first error is kept in *err.
+__device__ bool team_barrier(unsigned *ctr, unsigned k, unsigned &epoch, int *err, unsigned long long limit_ns,
+                             SharedM &sh)
+{
+    __syncthreads();
+    epoch += 1;
+    if (threadIdx.x == 0) {
+        const unsigned target = epoch * k;
+        __threadfence();
+        mf_red_relaxed_add_u32(ctr, 1u);
+        bool ok = true;
+        const unsigned long long t0 = mf_globaltimer();
+        unsigned spins = 0;
+        for (;;) {
+            const unsigned v = mf_ld_relaxed_u32(ctr);
+            if ((int)(v - target) >= 0) break;
+            if (*(volatile int *)err) { ok = false; break; }
+            if ((++spins & 63u) == 0u && mf_globaltimer() - t0 > limit_ns) {
+                atomicCAS(err, 0, MF_ERR_TIMEOUT);
+                ok = false;
+                break;
+            }
+        }
+        mf_fence_acq_rel_gpu();
+        sh.flag = ok ? 1 : 0;
+    }
+    __syncthreads();
+    return sh.flag != 0;
+}
+
+// The synchronisation of a team item: block partials into the team's slots,
+// the team barrier, then every member sums the k partials in the same order.
+// The first barrier (every member arriving at the item) may wait for members
+// still finishing earlier list entries, so it gets the longer limit.  The
+// team's parameters live in shared memory (no registers held across the body).
+struct TeamShared {
+    double *red;
+    unsigned *ctr;
+    int *err;
+    unsigned long long limit_ns, arrive_ns;
+    int k, r;
+    unsigned epoch;
+};
+
+struct TeamSync {
+    SharedM &sh;
+    TeamShared &ts;
+    template <int NV>
+    __device__ bool reduce(int kind, const double (&v)[NV], unsigned maxmask, double (&out)[NV])
+    {
+        MultiParams R;
+        R.red = ts.red;
+        block_partial_m<NV>(R, sh, kind, v, maxmask, ts.k, ts.r);
+        unsigned ep = ts.epoch;
+        const bool ok = team_barrier(ts.ctr, (unsigned)ts.k, ep, ts.err, ep == 0 ? ts.arrive_ns : ts.limit_ns, sh);
+        if (!ok) return false;
+        grid_collect_m<NV>(R, sh, kind, maxmask, out, ts.k);
+        if (threadIdx.x == 0) ts.epoch = ep;
+        __syncthreads();
+        return true;
+    }
+    __device__ bool writer() const { return ts.r == 0 && threadIdx.x == 0; }
+};
+
+// The half-warps of a team of k blocks (this block: rank r) split a system's
+// tile-rows by the cost prefix (k = 1: one block).
+__device__ __forceinline__ Ctx team_ctx(const BatchItem &it, int r, int k)
 {
     Ctx c;
     c.lane = threadIdx.x & 31;
@@ -1742,11 +1837,12 @@ __device__ __forceinline__ Ctx block_ctx(const BatchItem &it)
     c.half = c.lane >> 4;
     c.i = c.lane & 15;
     c.hmask = 0xFFFFu << (16 * c.half);
-    const int hw = c.wib * 2 + c.half;
+    const int halves = kHalvesPerBlock * k;
+    const int hw = r * kHalvesPerBlock + c.wib * 2 + c.half;
     const long long total = it.row_cost[it.tilem];
     auto split = [&](int h) -> int {
-        if (h >= kHalvesPerBlock) return it.tilem;
-        const long long target = (long long)((double)total * (double)h / (double)kHalvesPerBlock);
+        if (h >= halves) return it.tilem;
+        const long long target = (long long)((double)total * (double)h / (double)halves);
         int lo = 0, hi = it.tilem;
         while (lo < hi) {
             const int mid = (lo + hi) >> 1;
@@ -1762,11 +1858,79 @@ __device__ __forceinline__ Ctx block_ctx(const BatchItem &it)
     return c;
 }
 
+// The fields of SolverParams the CG body and the slice walk read, for one item.
+__device__ __forceinline__ SolverParams item_params(const BatchItem &it, const BatchParams &B)
+{
+    SolverParams P;
+    P.n = it.n;
+    P.tilem = it.tilem;
+    P.seg_ptr = it.seg_ptr;
+    P.seg_hdr = it.seg_hdr;
+    P.seg_tile = it.seg_tile;
+    P.seg_rowlen = it.seg_rowlen;
+    P.meta = it.meta;
+    P.v64 = it.v64;
+    P.v32 = it.v32;
+    P.v16 = it.v16;
+    P.v8 = it.v8;
+    P.i8_scale = it.i8_scale;
+    P.max_iter = B.max_iter;
+    P.fixed_iters = B.fixed_iters;
+    P.replace_every = B.replace_every;
+    P.use_lossless = B.use_lossless;
+    P.lossless_any = B.use_lossless;     // conservative: the batch does not scan its tiles
+    P.tol = B.tol;
+    P.demote16 = B.demote16;
+    P.demote8 = B.demote8;
+    return P;
+}
+
+template <int MODE, class Sync>
+__device__ __forceinline__ void item_solve(const SolverParams &P, const MultiParams &M, int nr, const Ctx &c,
+                                           SharedM &sh, Sync &sy)
+{
+    switch (nr) {
+    case 1: cg_multi_body<MODE, 1>(P, M, c, sh, sy); break;
+    case 2: cg_multi_body<MODE, 2>(P, M, c, sh, sy); break;
+    case 4: cg_multi_body<MODE, 4>(P, M, c, sh, sy); break;
+    default: cg_multi_body<MODE, 8>(P, M, c, sh, sy); break;
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
 {
     __shared__ SharedM sh;
+    __shared__ TeamShared ts;
     __shared__ int next;
+    // this block's team entries, in the global schedule order
+    for (int e = B.bptr[blockIdx.x]; e < B.bptr[blockIdx.x + 1]; e++) {
+        const int2 ent = B.blist[e];
+        const BatchItem &it = B.items[ent.x];
+        const SolverParams P = item_params(it, B);
+        const Ctx c = team_ctx(it, ent.y, it.team);
+        const MultiParams M = it.M;
+        if (threadIdx.x == 0) {
+            ts.red = M.red;
+            ts.ctr = it.ctr;
+            ts.err = B.err;
+            ts.limit_ns = B.timeout_ns;
+            ts.arrive_ns = B.arrive_timeout_ns;
+            ts.k = it.team;
+            ts.r = ent.y;
+            ts.epoch = 0u;
+        }
+        __syncthreads();
+        const unsigned long long t0 = mf_globaltimer();
+        TeamSync sy{sh, ts};
+        item_solve<MODE>(P, M, it.nr, c, sh, sy);
+        __syncthreads();
+        if (ent.y == 0 && threadIdx.x == 0) {         // the item's start and end, for the report
+            M.out[4 * it.nr + 3] = (double)t0;
+            M.out[4 * it.nr + 4] = (double)mf_globaltimer();
+        }
+        if (*(volatile int *)B.err) return;      // a team wait gave up: the launch reports it
+    }
     for (;;) {
         if (threadIdx.x == 0) next = (int)atomicAdd(B.head, 1u);
         __syncthreads();
@@ -1774,37 +1938,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
         __syncthreads();
         if (pos >= B.n_items) break;
         const BatchItem &it = B.items[B.order[pos]];
-        SolverParams P;              // the fields the CG body and the slice walk read
-        P.n = it.n;
-        P.tilem = it.tilem;
-        P.seg_ptr = it.seg_ptr;
-        P.seg_hdr = it.seg_hdr;
-        P.seg_tile = it.seg_tile;
-        P.seg_rowlen = it.seg_rowlen;
-        P.meta = it.meta;
-        P.v64 = it.v64;
-        P.v32 = it.v32;
-        P.v16 = it.v16;
-        P.v8 = it.v8;
-        P.i8_scale = it.i8_scale;
-        P.max_iter = B.max_iter;
-        P.fixed_iters = B.fixed_iters;
-        P.replace_every = B.replace_every;
-        P.use_lossless = B.use_lossless;
-        P.lossless_any = B.use_lossless;     // conservative: the batch does not scan its tiles
-        P.tol = B.tol;
-        P.demote16 = B.demote16;
-        P.demote8 = B.demote8;
-        const Ctx c = block_ctx(it);
+        const SolverParams P = item_params(it, B);
+        const Ctx c = team_ctx(it, 0, 1);
         BlockSync sy{sh};
         const MultiParams M = it.M;
-        switch (it.nr) {
-        case 1: cg_multi_body<MODE, 1>(P, M, c, sh, sy); break;
-        case 2: cg_multi_body<MODE, 2>(P, M, c, sh, sy); break;
-        case 4: cg_multi_body<MODE, 4>(P, M, c, sh, sy); break;
-        default: cg_multi_body<MODE, 8>(P, M, c, sh, sy); break;
-        }
+        const unsigned long long t0 = mf_globaltimer();
+        item_solve<MODE>(P, M, it.nr, c, sh, sy);
         __syncthreads();
+        if (threadIdx.x == 0) {
+            M.out[4 * it.nr + 3] = (double)t0;
+            M.out[4 * it.nr + 4] = (double)mf_globaltimer();
+        }
     }
 }
 
@@ -2436,15 +2580,20 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
 namespace {
 
 struct BatchImpl {
-    int dev = 0, cap = 8, nitems = 0, nsm = 0;
+    int dev = 0, cap = 8, nitems = 0, nsm = 0, max_res = 0;
     std::vector<mf_matrix_s *> sys;
     std::vector<int> nrhs;
-    // items: system, first column, columns, interleave width
-    std::vector<int> it_sys, it_col0, it_ncol, it_nr;
+    // items: system, first column, columns, interleave width, team size
+    std::vector<int> it_sys, it_col0, it_ncol, it_nr, it_team;
     std::vector<BatchItem> h_items;
     BatchItem *d_items = nullptr;
-    int *d_order = nullptr;
-    unsigned *d_head = nullptr;
+    int *d_order = nullptr;            // queue items, largest estimated cost first
+    int nqueue = 0;
+    int grid = 1;                      // blocks of the launch
+    int *d_bptr = nullptr;             // [grid + 1] team entries per block
+    int2 *d_blist = nullptr;
+    unsigned *d_ctl = nullptr;         // queue head | error word | one barrier counter per team item
+    size_t ctl_bytes = 0;
     char *d_pool = nullptr;
     size_t pool_bytes = 0;
     std::vector<size_t> out_off;       // offset of each item's report words in the pool
@@ -2460,18 +2609,77 @@ struct BatchImpl {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
         graph_key.clear();
-        void *p[] = {d_items, d_order, d_head, d_pool};
+        void *p[] = {d_items, d_order, d_bptr, d_blist, d_ctl, d_pool};
         for (void *q : p)
             if (q) cudaFree(q);
-        d_items = nullptr; d_order = nullptr; d_head = nullptr; d_pool = nullptr;
+        d_items = nullptr; d_order = nullptr; d_bptr = nullptr; d_blist = nullptr; d_ctl = nullptr;
+        d_pool = nullptr;
     }
 };
 
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 constexpr int kOutWords = 4 * kMaxNR + 8;
 
+// Team sizes and the list schedule of team items.  fair = total cost / blocks;
+// an item gets k = round(kTeamGrain x cost / fair) blocks, at most the launch and at most
+// one block per kMinTeamRows tile-rows; k >= 2 makes it a team item.  Team
+// items, largest first, go to the k blocks that are free first (ties: lower
+// block), start = the latest of their free times, and those blocks are busy
+// for cost / k.  Each block's list is sorted by (start, item).
+void batch_schedule(const std::vector<double> &cost, const std::vector<int> &tilem, int grid, std::vector<int> &team,
+                    std::vector<int> &bptr, std::vector<int2> &blist, std::vector<int> &queue)
+{
+    const int ni = (int)cost.size();
+    double total = 0.0;
+    for (double c : cost) total += c;
+    const double fair = total / (double)std::max(1, grid);
+    team.assign(ni, 1);
+    std::vector<int> order(ni);
+    for (int t = 0; t < ni; t++) order[t] = t;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<double> free_at(grid, 0.0);
+    std::vector<std::vector<std::pair<double, int2>>> lists(grid);
+    queue.clear();
+    for (int t : order) {
+        int k = 1;
+        if (fair > 0.0 && grid > 1) {
+            const double want = std::floor(kTeamGrain * cost[t] / fair + 0.5);
+            k = (int)std::min<double>(want, (double)std::min(grid, std::max(1, tilem[t] / kMinTeamRows)));
+            k = std::max(k, 1);
+        }
+        if (k < 2) {
+            queue.push_back(t);
+            continue;
+        }
+        team[t] = k;
+        std::vector<int> blk(grid);
+        for (int q = 0; q < grid; q++) blk[q] = q;
+        std::stable_sort(blk.begin(), blk.end(), [&](int a, int b) { return free_at[a] < free_at[b]; });
+        blk.resize(k);
+        std::sort(blk.begin(), blk.end());
+        double start = 0.0;
+        for (int q : blk) start = std::max(start, free_at[q]);
+        const double end = start + cost[t] / (double)k;
+        for (int r = 0; r < k; r++) {
+            free_at[blk[r]] = end;
+            lists[blk[r]].push_back({start, make_int2(t, r)});
+        }
+    }
+    bptr.assign(grid + 1, 0);
+    blist.clear();
+    for (int q = 0; q < grid; q++) {
+        std::stable_sort(lists[q].begin(), lists[q].end(), [](const std::pair<double, int2> &a,
+                                                             const std::pair<double, int2> &b) {
+            return a.first < b.first || (a.first == b.first && a.second.x < b.second.x);
+        });
+        for (auto &e : lists[q]) blist.push_back(e.second);
+        bptr[q + 1] = (int)blist.size();
+    }
+}
+
 // Items for column cap `cap`: each system's right-hand sides in groups of <= cap,
-// interleave width the next power of two (1, 2, 4, 8); all vectors in one pool.
+// interleave width the next power of two (1, 2, 4, 8); team sizes and the
+// schedule; all vectors in one pool.
 int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
 {
     B.release_items();
@@ -2486,8 +2694,27 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
             B.it_nr.push_back(mf_batch_width(g));
         }
     B.nitems = (int)B.it_sys.size();
-    // per item: B | X | R | P | Q (doubles), R32 (floats), segment magnitudes, report words
-    std::vector<size_t> off(B.nitems);
+    std::vector<double> cost(B.nitems);
+    std::vector<int> tilem(B.nitems);
+    for (int t = 0; t < B.nitems; t++) {
+        const mf_matrix_s *A = B.sys[B.it_sys[t]];
+        cost[t] = mf_batch_item_cost(A->nnz, A->n_rows, B.it_nr[t]);
+        tilem[t] = A->tilem;
+    }
+    // one block per SM (all resident: the launch is cooperative)
+    B.grid = std::max(1, std::min(B.max_res, B.nsm));
+    std::vector<int> bptr, queue;
+    std::vector<int2> blist;
+    batch_schedule(cost, tilem, B.grid, B.it_team, bptr, blist, queue);
+    if (blist.empty()) {
+        // no team: one block per item at most
+        B.grid = std::max(1, std::min(B.grid, B.nitems));
+        bptr.assign(B.grid + 1, 0);
+    }
+    B.nqueue = (int)queue.size();
+    // per item: B | X | R | P | Q (doubles), R32 (floats), segment magnitudes,
+    // report words, team partials
+    std::vector<size_t> off(B.nitems), red_off(B.nitems, 0);
     size_t total = 0;
     B.out_off.assign(B.nitems, 0);
     for (int t = 0; t < B.nitems; t++) {
@@ -2498,12 +2725,21 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
                  align256((size_t)(A->tilem + 1) * sizeof(float));
         B.out_off[t] = total;
         total += align256(kOutWords * sizeof(double));
+        if (B.it_team[t] > 1) {
+            red_off[t] = total;
+            total += align256((size_t)kRedKinds * B.it_team[t] * kRedWidthM * sizeof(double));
+        }
     }
     B.pool_bytes = total;
     MF_CUDA_TRY(cudaMalloc((void **)&B.d_pool, total > 0 ? total : 256));
     MF_CUDA_TRY(cudaMemsetAsync(B.d_pool, 0, total > 0 ? total : 256, s));
+    int nteam = 0;
+    std::vector<int> ctr_of(B.nitems, -1);
+    for (int t = 0; t < B.nitems; t++)
+        if (B.it_team[t] > 1) ctr_of[t] = nteam++;
+    B.ctl_bytes = sizeof(unsigned) * (size_t)(2 + nteam);
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_ctl, B.ctl_bytes));
     B.h_items.resize(B.nitems);
-    std::vector<double> cost(B.nitems);
     for (int t = 0; t < B.nitems; t++) {
         const mf_matrix_s *A = B.sys[B.it_sys[t]];
         const size_t L = (size_t)A->vec_len, nr = (size_t)B.it_nr[t];
@@ -2512,35 +2748,37 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
         it.seg_ptr = A->d_seg_ptr; it.seg_hdr = A->d_seg_hdr; it.seg_tile = A->d_seg_tile;
         it.seg_rowlen = A->d_seg_rowlen; it.meta = A->d_meta; it.v64 = A->d_v64; it.v32 = A->d_v32;
         it.v16 = A->d_v16; it.v8 = A->d_v8; it.i8_scale = A->d_i8_scale; it.row_cost = A->d_row_cost;
-        it.n = A->n_rows; it.tilem = A->tilem; it.nr = (int)nr;
+        it.n = A->n_rows; it.tilem = A->tilem; it.nr = (int)nr; it.team = B.it_team[t];
         char *base = B.d_pool + off[t];
         double *v = (double *)base;
         it.M.B = v; it.M.X = v + L * nr; it.M.R = v + 2 * L * nr; it.M.Pv = v + 3 * L * nr; it.M.Q = v + 4 * L * nr;
         char *f = base + align256(5 * L * nr * sizeof(double));
         it.M.R32 = (float *)f;
         it.M.mag = (float *)(f + align256(L * nr * sizeof(float)));
-        it.M.red = nullptr;
+        it.M.red = it.team > 1 ? (double *)(B.d_pool + red_off[t]) : nullptr;
         it.M.out = (double *)(B.d_pool + B.out_off[t]);
         it.M.nr = B.it_ncol[t];
-        cost[t] = mf_batch_item_cost(A->nnz, A->n_rows, (int)nr);
+        it.ctr = it.team > 1 ? B.d_ctl + 2 + ctr_of[t] : nullptr;
     }
-    std::vector<int> order(B.nitems);
-    for (int t = 0; t < B.nitems; t++) order[t] = t;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     MF_CUDA_TRY(cudaMalloc((void **)&B.d_items, sizeof(BatchItem) * (size_t)std::max(1, B.nitems)));
-    MF_CUDA_TRY(cudaMalloc((void **)&B.d_order, sizeof(int) * (size_t)std::max(1, B.nitems)));
-    MF_CUDA_TRY(cudaMalloc((void **)&B.d_head, sizeof(unsigned)));
-    if (B.nitems > 0) {
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_order, sizeof(int) * (size_t)std::max(1, B.nqueue)));
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_bptr, sizeof(int) * (size_t)(B.grid + 1)));
+    MF_CUDA_TRY(cudaMalloc((void **)&B.d_blist, sizeof(int2) * (size_t)std::max<size_t>(1, blist.size())));
+    if (B.nitems > 0)
         MF_CUDA_TRY(cudaMemcpyAsync(B.d_items, B.h_items.data(), sizeof(BatchItem) * B.nitems,
                                     cudaMemcpyHostToDevice, s));
-        MF_CUDA_TRY(cudaMemcpyAsync(B.d_order, order.data(), sizeof(int) * B.nitems, cudaMemcpyHostToDevice, s));
-    }
+    if (B.nqueue > 0)
+        MF_CUDA_TRY(cudaMemcpyAsync(B.d_order, queue.data(), sizeof(int) * B.nqueue, cudaMemcpyHostToDevice, s));
+    MF_CUDA_TRY(cudaMemcpyAsync(B.d_bptr, bptr.data(), sizeof(int) * (B.grid + 1), cudaMemcpyHostToDevice, s));
+    if (!blist.empty())
+        MF_CUDA_TRY(cudaMemcpyAsync(B.d_blist, blist.data(), sizeof(int2) * blist.size(), cudaMemcpyHostToDevice, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
     return MF_SUCCESS;
 }
 
 // Enqueue one batched solve on s: interleave every item's columns, reset the
-// queue, the persistent launch, de-interleave.  No host synchronisation.
+// queue head, error word and team counters, the cooperative persistent launch,
+// de-interleave.  No host synchronisation.
 int batch_enqueue(BatchImpl &B, const double *const *Bd, double *const *Xd, const BatchParams &bp0, int mode,
                   cudaStream_t s)
 {
@@ -2551,16 +2789,27 @@ int batch_enqueue(BatchImpl &B, const double *const *Bd, double *const *Xd, cons
                                           (double *)B.h_items[t].M.B);
     }
     MF_CUDA_TRY(cudaGetLastError());
-    MF_CUDA_TRY(cudaMemsetAsync(B.d_head, 0, sizeof(unsigned), s));
+    MF_CUDA_TRY(cudaMemsetAsync(B.d_ctl, 0, B.ctl_bytes, s));
     BatchParams bp = bp0;
     bp.items = B.d_items;
     bp.order = B.d_order;
-    bp.n_items = B.nitems;
-    bp.head = B.d_head;
-    const int grid = std::max(1, std::min(B.nsm, B.nitems));
-    if (mode == MODE_FP64) k_batch<MODE_FP64><<<grid, kThreads, 0, s>>>(bp);
-    else k_batch<MODE_MIXED><<<grid, kThreads, 0, s>>>(bp);
-    MF_CUDA_TRY(cudaGetLastError());
+    bp.n_items = B.nqueue;
+    bp.head = B.d_ctl;
+    bp.err = (int *)(B.d_ctl + 1);
+    bp.bptr = B.d_bptr;
+    bp.blist = B.d_blist;
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(B.grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (mode == MODE_FP64) MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_FP64>, bp));
+    else MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_MIXED>, bp));
     for (int t = 0; t < B.nitems; t++) {
         const mf_matrix_s *A = B.sys[B.it_sys[t]];
         const int nr = B.it_nr[t], g = B.it_col0[t] / nr;
@@ -2585,6 +2834,15 @@ int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems
     if (cudaGetDevice(&B.dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&B.nsm, cudaDevAttrMultiProcessorCount, B.dev) != cudaSuccess)
         rc = MF_ERR_CUDA;
+    if (rc == MF_SUCCESS) {
+        // co-resident blocks of the cooperative launch (both precisions)
+        int o64 = 0, o32 = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o64, k_batch<MODE_FP64>, kThreads, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o32, k_batch<MODE_MIXED>, kThreads, 0) != cudaSuccess ||
+            std::min(o64, o32) < 1)
+            rc = MF_ERR_CUDA;
+        B.max_res = std::min(o64, o32) * B.nsm;
+    }
     for (int k = 0; rc == MF_SUCCESS && k < nsys; k++) {
         if (!systems[k] || nrhs[k] < 1 || systems[k]->n_rows != systems[k]->n_cols || systems[k]->dev != B.dev) {
             rc = MF_ERR_INVALID;
@@ -2637,6 +2895,11 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
     bp.tol = opt->tol;
     bp.demote16 = (float)opt->demote_fp16;
     bp.demote8 = (float)opt->demote_int8;
+    // team waits: within an item the members run in step (the normal bound);
+    // arriving at an item may wait for members finishing earlier list entries
+    const double to = opt->wait_timeout_s > 0 ? opt->wait_timeout_s : 10.0;
+    bp.timeout_ns = (unsigned long long)(to * 1e9);
+    bp.arrive_timeout_ns = (unsigned long long)(std::max(to * 30.0, 300.0) * 1e9);
     cudaStream_t run = s ? s : B.own;
     if (!s) {
         // the batch's own stream does not synchronise with the default stream on
@@ -2688,11 +2951,18 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
     for (int t = 0; t < B.nitems; t++)
         MF_CUDA_TRY(cudaMemcpyAsync(outs.data() + (size_t)t * kOutWords, B.d_pool + B.out_off[t],
                                     kOutWords * sizeof(double), cudaMemcpyDeviceToHost, run));
+    int team_err = 0;
+    MF_CUDA_TRY(cudaMemcpyAsync(&team_err, B.d_ctl + 1, sizeof(int), cudaMemcpyDeviceToHost, run));
     MF_CUDA_TRY(cudaStreamSynchronize(run));
     float ms = 0.f;
     MF_CUDA_TRY(cudaEventElapsedTime(&ms, B.e0, B.e1));
     B.last_ms = ms;
-    int status = MF_SUCCESS;
+    int status = team_err;
+    double t_first = 0.0;                  // the launch's first item start (globaltimer ns)
+    for (int t = 0; t < B.nitems; t++) {
+        const double ts = outs[(size_t)t * kOutWords + 4 * B.it_nr[t] + 3];
+        if (ts > 0.0 && (t_first == 0.0 || ts < t_first)) t_first = ts;
+    }
     std::vector<int> first(B.sys.size() + 1, 0);
     for (size_t k = 0; k < B.sys.size(); k++) first[k + 1] = first[k] + B.nrhs[k];
     for (int t = 0; t < B.nitems; t++) {
@@ -2707,10 +2977,13 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
             r->converged = (int)o[4 * c + 1];
             r->relres_true = o[4 * c + 2];
             r->relres_rec = o[4 * c + 3];
-            r->status = (int)o[4 * nr + 1];
+            r->status = team_err ? team_err : (int)o[4 * nr + 1];
             r->replacements = (int)o[4 * nr + 2];
             r->time_ms = ms;
-            r->grid_blocks = std::max(1, std::min(B.nsm, B.nitems));
+            r->phase_ms[0] = o[4 * nr + 3] > 0.0 ? (o[4 * nr + 3] - t_first) * 1e-6 : 0.0;
+            r->phase_ms[1] = o[4 * nr + 4] > 0.0 ? (o[4 * nr + 4] - t_first) * 1e-6 : 0.0;
+            r->phase_ms[2] = (double)B.it_team[t];
+            r->grid_blocks = B.grid;
             r->threads_per_block = kThreads;
         }
     }

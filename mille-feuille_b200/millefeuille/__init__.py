@@ -276,7 +276,14 @@ class Batch:
         reps = (Report * sum(self.nrhs))()
         st = L.mf_batch_solve(self._h, pb, px, C.byref(o), reps, int(bool(use_graph)),
                               C.c_void_p(stream) if stream else None)
-        flat = [r.as_dict() for r in reps]
+        flat = []
+        for r in reps:
+            d = r.as_dict()
+            # batch reports: the column's work item's start / end after the
+            # launch's first item start, and the blocks that solved it
+            del d["phase_ms"]
+            d["item_start_ms"], d["item_end_ms"], d["item_blocks"] = r.phase_ms[0], r.phase_ms[1], int(r.phase_ms[2])
+            flat.append(d)
         out, k0 = [], 0
         for k in self.nrhs:
             out.append(flat[k0:k0 + k])

@@ -75,10 +75,9 @@ def test_batch_rejects_bad_input(mf, cuda, systems):
 
 def test_batch_split_over_parts_matches_one_batch(mf, cuda, systems):
     """The multi-GPU split run part by part on one GPU (each part its own
-    mf_batch, as each rank would): every system's solution is bitwise the one
-    the single batch gives (an item's arithmetic does not depend on the block,
-    the launch or the other items)."""
-    import torch
+    mf_batch, as each rank would): every system converges and agrees with the
+    single batch (a part may give an item a different team size, so the
+    reduction order, and with it the last digits, can differ)."""
     from millefeuille import shard
     mats, Bs = _setup(mf, systems)
     nr = [B.shape[0] for B in Bs]
@@ -90,5 +89,36 @@ def test_batch_split_over_parts_matches_one_batch(mf, cuda, systems):
         Xq, rq = mf.Batch([mats[k] for k in own], [nr[k] for k in own]).solve(
             [Bs[k] for k in own], method="cg", precision="mixed", tol=1e-8, use_graph=False)
         for k, X, rk in zip(own, Xq, rq):
-            assert torch.equal(X, X1[k])
-            assert [x["iterations"] for x in rk] == [x["iterations"] for x in r1[k]]
+            A, B = systems[k][2], systems[k][3]
+            x1 = X1[k].cpu().numpy()
+            x = X.cpu().numpy()
+            for c in range(B.shape[0]):
+                assert rk[c]["converged"] and _relres(A, x[c], B[c]) <= 1.0001e-8
+            np.testing.assert_allclose(x, x1, rtol=0, atol=1e-4 * np.abs(x1).max())
+
+
+def test_batch_team_items(mf, cuda):
+    """An item far above a fair share of the launch (one 27-point system of
+    64,000 unknowns with 8 right-hand sides next to small ones) is solved by a
+    team of blocks: every column converges on its FP64 true residual, the large
+    system agrees with a single-system FP64 solve, and a replay from a CUDA
+    graph (a cooperative launch in the graph) is bitwise the direct launch."""
+    import torch
+    from millefeuille import matrices as M
+    big = M.batch_systems(1, seed=11, side2d=(256, 256), side3d=(40, 40), rhs=(8, 8))
+    small = M.batch_systems(6, seed=12, side2d=(8, 24), side3d=(4, 8), rhs=(1, 4))
+    systems = big + small
+    mats, Bs = _setup(mf, systems)
+    batch = mf.Batch(mats, [B.shape[0] for B in Bs])
+    X0, r0 = batch.solve(Bs, method="cg", precision="mixed", tol=1e-8, use_graph=False)
+    Xg, rg = batch.solve(Bs, method="cg", precision="mixed", tol=1e-8, use_graph=True)
+    Xh, rh = batch.solve(Bs, method="cg", precision="mixed", tol=1e-8, use_graph=True)
+    for a, b, c in zip(X0, Xg, Xh):
+        assert torch.equal(a, b) and torch.equal(a, c)
+    assert r0[0][0]["grid_blocks"] > 1
+    for (kind, side, A, B), X, rk, G in zip(systems, X0, r0, mats):
+        X = X.cpu().numpy()
+        for c in range(B.shape[0]):
+            assert rk[c]["converged"] and _relres(A, X[c], B[c]) <= 1.0001e-8, (kind, side, c, rk[c])
+    xs, _ = mats[0].solve(systems[0][3][0], method="cg", precision="fp64", tol=1e-12)
+    np.testing.assert_allclose(X0[0].cpu().numpy()[0], xs, rtol=0, atol=1e-5 * np.abs(xs).max())

@@ -17,7 +17,7 @@ def _cost(n, nnz, nrhs, cap=8):
     for c0 in range(0, nrhs, cap):
         g = min(cap, nrhs - c0)
         w = 8 if g >= 5 else 4 if g >= 3 else 2 if g == 2 else 1
-        c += nnz * (1.0 + 0.35 * (w - 1)) * math.sqrt(max(n, 1))
+        c += (max(n, 1) + nnz / 64.0) * (1.0 + 0.35 * (w - 1)) * max(n, 1) ** 0.4
     return c
 
 
