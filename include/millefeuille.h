@@ -270,17 +270,16 @@ int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_p
  *    MF_PREC_FP64 or MF_PREC_MIXED (every tile in FP32), as for mf_spmv.
  *  - The call is asynchronous on `stream` (NULL: default stream); y is ready
  *    when the stream reaches that point.
- *  - Scratch: the padded copy of x (and its FP32 shadow) lives in a fixed
- *    device buffer compiled into the library, MF_SPMV_NOALLOC_MAX_LEN entries
- *    (16 MB + 8 MB per device).  Matrices whose padded vector length,
+ *  - Scratch: the padded copy of x lives in a fixed device buffer compiled
+ *    into the library, MF_SPMV_NOALLOC_MAX_LEN doubles (16 MB per device).  Matrices whose padded vector length,
  *    16 * ceil(max(n_rows, n_cols) / 16), exceeds it are rejected with
  *    MF_ERR_UNSUPPORTED before anything is launched.
  *  - Nothing has to start at zero: each call writes every scratch entry the
  *    kernel reads (x, then zeros up to the padded length).
  *  - The first call on a device looks the buffer up (cudaGetSymbolAddress,
  *    which may load the library's device code); make that first call before
- *    any stream capture.  Later calls only issue a memset, a copy and the
- *    kernel(s).
+ *    any stream capture.  Later calls only issue a copy, a memset and the
+ *    kernel.
  *  - One buffer per device is shared by all handles and threads: calls on
  *    the same device must not overlap in time (issue them on one stream, or
  *    order the streams), otherwise they race on the scratch.
