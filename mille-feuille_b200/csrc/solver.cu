@@ -1766,6 +1766,7 @@ struct BatchParams {
     const int2 *blist;            // (item, rank in its team)
     int *err;                     // first error of a team wait (zeroed before the launch)
     unsigned long long timeout_ns, arrive_timeout_ns;
+    int stall_first;              // test hook: a team's first barrier expects one extra arrival
     int max_iter, fixed_iters, replace_every, use_lossless;
     double tol;
     float demote16, demote8;
@@ -1814,12 +1815,12 @@ struct BlockSync {
 // by `limit_ns`; a timeout, or an error set elsewhere, returns false and the
 // first error is kept in *err.
 __device__ bool team_barrier(unsigned *ctr, unsigned k, unsigned &epoch, int *err, unsigned long long limit_ns,
-                             SharedM &sh)
+                             SharedM &sh, int stall = 0)
 {
     __syncthreads();
     epoch += 1;
     if (threadIdx.x == 0) {
-        const unsigned target = epoch * k;
+        const unsigned target = epoch * k + ((stall && epoch == 1) ? 1u : 0u);
         __threadfence();
         mf_red_relaxed_add_u32(ctr, 1u);
         bool ok = true;
@@ -1854,6 +1855,7 @@ struct TeamShared {
     unsigned long long limit_ns, arrive_ns;
     int k, r;
     unsigned epoch;
+    int stall;
 };
 
 struct TeamSync {
@@ -1866,7 +1868,8 @@ struct TeamSync {
         R.red = ts.red;
         block_partial_m<NV>(R, sh, kind, v, maxmask, ts.k, ts.r);
         unsigned ep = ts.epoch;
-        const bool ok = team_barrier(ts.ctr, (unsigned)ts.k, ep, ts.err, ep == 0 ? ts.arrive_ns : ts.limit_ns, sh);
+        const bool ok =
+            team_barrier(ts.ctr, (unsigned)ts.k, ep, ts.err, ep == 0 ? ts.arrive_ns : ts.limit_ns, sh, ts.stall);
         if (!ok) return false;
         grid_collect_m<NV>(R, sh, kind, maxmask, out, ts.k);
         if (threadIdx.x == 0) ts.epoch = ep;
@@ -1968,6 +1971,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
             ts.k = it.team;
             ts.r = ent.y;
             ts.epoch = 0u;
+            ts.stall = B.stall_first;
         }
         __syncthreads();
         const unsigned long long t0 = mf_globaltimer();
@@ -2936,6 +2940,12 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
     const double to = opt->wait_timeout_s > 0 ? opt->wait_timeout_s : 10.0;
     bp.timeout_ns = (unsigned long long)(to * 1e9);
     bp.arrive_timeout_ns = (unsigned long long)(std::max(to * 30.0, 300.0) * 1e9);
+    if (opt->test_stall_barrier) {
+        // test hook: every team's first barrier waits for an arrival that never
+        // comes and gives up after wait_timeout_s (MF_ERR_TIMEOUT, no fault)
+        bp.stall_first = 1;
+        bp.arrive_timeout_ns = bp.timeout_ns;
+    }
     cudaStream_t run = s ? s : B.own;
     if (!s) {
         // the batch's own stream does not synchronise with the default stream on
@@ -2951,7 +2961,8 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
             key.push_back(Xd[k]);
         }
         const double opts[] = {opt->tol, (double)opt->max_iter, (double)opt->fixed_iters, (double)opt->replace_every,
-                               opt->demote_fp16, opt->demote_int8, (double)opt->use_lossless, (double)B.cap};
+                               opt->demote_fp16, opt->demote_int8, (double)opt->use_lossless, (double)B.cap,
+                               opt->wait_timeout_s, (double)opt->test_stall_barrier};
         for (double v : opts) {
             unsigned long long u;
             memcpy(&u, &v, sizeof(u));

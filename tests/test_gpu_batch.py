@@ -122,3 +122,26 @@ def test_batch_team_items(mf, cuda):
             assert rk[c]["converged"] and _relres(A, X[c], B[c]) <= 1.0001e-8, (kind, side, c, rk[c])
     xs, _ = mats[0].solve(systems[0][3][0], method="cg", precision="fp64", tol=1e-12)
     np.testing.assert_allclose(X0[0].cpu().numpy()[0], xs, rtol=0, atol=1e-5 * np.abs(xs).max())
+
+
+def test_batch_team_wait_timeout_is_reported(mf, cuda):
+    """Failure detection on the team path without a GPU fault: with the test
+    hook every team's first barrier waits for an arrival that never comes; the
+    bounded wait gives up after wait_timeout_s, the batch returns
+    MF_ERR_TIMEOUT, and the same batch then solves normally (the context stays
+    usable)."""
+    from millefeuille import matrices as M
+    systems = M.batch_systems(1, seed=11, side2d=(256, 256), side3d=(40, 40), rhs=(8, 8)) + \
+        M.batch_systems(3, seed=12, side2d=(8, 24), side3d=(4, 8), rhs=(1, 4))
+    mats, Bs = _setup(mf, systems)
+    batch = mf.Batch(mats, [B.shape[0] for B in Bs])
+    o = mf.default_options(precision="mixed", tol=1e-8, wait_timeout_s=0.5, test_stall_barrier=1)
+    with pytest.raises(mf.MFError) as e:
+        batch.solve(Bs, options=o, use_graph=False)
+    assert e.value.status == 4                      # MF_ERR_TIMEOUT
+    assert e.value.report[0][0]["item_blocks"] > 1
+    X, r = batch.solve(Bs, method="cg", precision="mixed", tol=1e-8, use_graph=False)
+    for (kind, side, A, B), Xk, rk in zip(systems, X, r):
+        Xk = Xk.cpu().numpy()
+        for c in range(B.shape[0]):
+            assert rk[c]["converged"] and _relres(A, Xk[c], B[c]) <= 1.0001e-8
