@@ -245,6 +245,8 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": alg},
         "clocks": clk.summary(),
     }
+    if not args.no_bicgstab:
+        out["config"]["bicgstab"] = bicgstab_line(dev, args.steps)
     if not args.no_adjoint:
         out["config"]["fwd_adjoint"] = fwd_adjoint(dev, args.adjoint_rhs)
     if not args.no_batch:
@@ -307,6 +309,37 @@ def batch_line(dev, nsys, rank=0, world=1):
         out["split"] = {"gpus": world, "systems_per_gpu": [part.count(q) for q in range(world)],
                         "estimated_load_imbalance": round(max(loads) / (sum(loads) / world), 3),
                         "rhs_per_item_rank0": cap}
+    return out
+
+
+def bicgstab_line(dev, steps):
+    """The reference's second solver on its own workload: BiCGSTAB on the
+    nonsymmetric 3D convection-diffusion system on 96^3 (upwind, v = 10 (sin y,
+    sin z, sin x), b = A 1 + 0.01 N(0,1), seed 2), mixed precision and FP64 to
+    relres 1e-8, FP64 residual replacement every 50 iterations in mixed mode.
+    One untimed solve each, then the best of `steps` (CUDA-event kernel time)."""
+    import numpy as np
+    import torch
+    import millefeuille as mf
+    from millefeuille import matrices as M
+    A, b, pe = M.convdiff3d(96, seed=2)
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    bd = torch.from_numpy(b).to(dev)
+    xd = torch.zeros_like(bd)
+    out = {"workload": f"convdiff3d_96 (n={A.n}, nnz={A.nnz}, max cell Peclet {pe:.2f}), BiCGSTAB tol 1e-8"}
+    for prec in ("mixed", "fp64"):
+        o = mf.default_options(method="bicgstab", precision=prec, tol=TOL, replace_every=50 if prec == "mixed" else 0)
+        G.solve(bd, xd, options=o)
+        best = None
+        for _ in range(max(1, steps)):
+            _, r = G.solve(bd, xd, options=o)
+            if best is None or r["time_ms"] < best["time_ms"]:
+                best = r
+        x = xd.cpu().numpy()
+        out[prec] = {"ms": round(best["time_ms"], 3), "iterations": best["iterations"],
+                     "relres_true": best["relres_true"],
+                     "relres_host_check": float(np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b))}
+    out["mixed_vs_fp64_speedup"] = round(out["fp64"]["ms"] / out["mixed"]["ms"], 3)
     return out
 
 
@@ -459,6 +492,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-solve (fwd+adjoint) line")
     ap.add_argument("--adjoint-rhs", type=int, default=32)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solves line")
+    ap.add_argument("--no-bicgstab", action="store_true", help="skip the BiCGSTAB (convection-diffusion) line")
     ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     args = ap.parse_args()

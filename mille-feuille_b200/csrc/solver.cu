@@ -914,7 +914,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             // ---- BiCGSTAB A1: v = A p, alpha = r1 / (rh.v) ----
             double prv = 0.0;
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
-                             make_x(P.p, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, invM), cnt,
+                             make_x(P.p, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, invM, dynA), cnt,
                              [&](int R, double y) {
                                  const int row = R * MF_BS + c.i;
                                  if (row < n) {
@@ -931,7 +931,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             alpha = r1 / v[0];
             if (!isfinite(alpha)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B1: s = r - alpha v ----
-            float smax = 0.0f;
+            float smax = 0.0f, smin = 3.0e38f;
             for (int R = c.rbeg; R < c.rend; R++) {
                 const int row = R * MF_BS + c.i;
                 const bool valid = row < n;
@@ -942,18 +942,20 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                     P.s[row] = sn;
                 }
                 publish_dir<MODE>(R, row, valid, sn, sold, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, smax, c.hmask,
-                                  true);
+                                  true, &smin);
             }
             clk.lap(PH_VECB);
-            block_partial(P, sh, 2, (double)smax, 0, 0, 0, 1, 0x1u);
+            // (max, -min) of s's segment magnitudes; only the mixed mode uses the minimum
+            block_partial(P, sh, 2, (double)smax, -(double)smin, 0, 0, kNvSeg - 1, 0x3u);
             if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 2, 1, 0x1u, v);
+            grid_collect(P, sh, 2, kNvSeg - 1, 0x3u, v);
             clk.lap(PH_BAR);
             invMs = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
+            const int dynS = (MODE == MODE_MIXED) ? dyn_of(v[0], v[1]) : 1;
             // ---- A2: t = A s, omega = (t.s)/(t.t) ----
             double pts = 0.0, ptt = 0.0;
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
-                             make_x(P.s, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, invMs), cnt,
+                             make_x(P.s, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, invMs, dynS), cnt,
                              [&](int R, double y) {
                                  const int row = R * MF_BS + c.i;
                                  if (row < n) {
@@ -1058,6 +1060,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
         }
         rr = rr_new;
         bmax = 0.0f;
+        float pmin = 3.0e38f;
         for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
             double pv[kVB], rv[kVB], xq[kVB];    // xq: x (CG, x not yet updated) or v (BiCGSTAB)
 #pragma unroll
@@ -1082,15 +1085,16 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                     if (bicg && restart) P.rh[row] = rv[u];
                 }
                 publish_dir<MODE>(R, row, valid, valid ? pn : 0.0, pold, P.p32, P.p16, P.p8, P.mag_p, P.lab_p,
-                                  bmax, c.hmask, true);
+                                  bmax, c.hmask, true, &pmin);
             }
         }
         clk.lap(PH_VECC);
-        block_partial(P, sh, 6, (double)bmax, 0, 0, 0, 1, 0x1u);
+        block_partial(P, sh, 6, (double)bmax, -(double)pmin, 0, 0, kNvSeg - 1, 0x3u);
         if (!grid_barrier(P, epoch, sh)) return;
-        grid_collect(P, sh, 6, 1, 0x1u, v);
+        grid_collect(P, sh, 6, kNvSeg - 1, 0x3u, v);
             clk.lap(PH_BAR);
         invM = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
+        if (MODE == MODE_MIXED) dynA = dyn_of(v[0], v[1]);
     }
     // ---- final FP64 true residual when the last one was not already formed ----
     if (!last_true) {
