@@ -214,3 +214,29 @@ def test_gpu_dropin_bicgstab(mf, cuda, cd3d, tmp_path, monkeypatch):
     assert rc == 0
     np.testing.assert_allclose(rhs, A.to_scipy() @ np.ones(A.n), rtol=1e-14)
     assert _relres(A, x, rhs) < 1e-6          # 50 fixed iterations on a well-conditioned system
+
+
+@pytest.mark.parametrize("method,precision", [("cg", "fp64"), ("cg", "mixed"), ("bicgstab", "fp64"),
+                                              ("bicgstab", "mixed")])
+def test_gpu_ragged_system_with_decoupled_rows(mf, oracle_mod, cuda, method, precision):
+    """A system whose size is not a multiple of 16 (the last tile-row is
+    partial) and whose last 40 rows are decoupled, diagonal-only (tiles holding
+    one entry per row): every method and precision converges on its FP64 true
+    residual, and the FP64 CG agrees with the oracle's CG."""
+    from millefeuille import matrices as M
+    import scipy.sparse as sp
+    L = M.laplace2d(31).to_scipy()                          # n = 961
+    D = sp.diags(np.linspace(1.0, 3.0, 40))
+    S = sp.block_diag([L, D]).tocsr()                       # n = 1001 = 62 * 16 + 9
+    S.sort_indices()
+    A = M.CSR(S.shape[0], S.indptr.astype(np.int32), S.indices.astype(np.int32), S.data.astype(np.float64))
+    b = np.random.default_rng(5).uniform(-1, 1, A.n)
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x, rep = G.solve(b, method=method, precision=precision, tol=1e-10)
+    assert rep["converged"] and rep["relres_true"] <= 1e-10
+    assert _relres(A, x, b) <= 1.0001e-10
+    if method == "cg" and precision == "fp64":
+        T = oracle_mod.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
+        xo, ro = T.cg_fp64(b, tol=1e-10, max_iter=5000)
+        np.testing.assert_allclose(x, xo, rtol=0, atol=1e-8 * np.abs(xo).max())
+        assert abs(rep["iterations"] - ro["iterations"]) <= 0.05 * ro["iterations"] + 1
