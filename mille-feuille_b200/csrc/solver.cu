@@ -319,20 +319,16 @@ __device__ __forceinline__ double slice_dot(const SolverParams &P, int4 h, int i
     // precision codes order FP64 < FP32 < FP16 < INT8: the minimum is the most precise
     int pr = MF_P64;
     if (!(MODE == MODE_FP64 || F64)) {
-        pr = (i < hdr_nt(h)) ? T.pr : MF_P8;
-#pragma unroll
-        for (int o = 8; o; o >>= 1) pr = min(pr, __shfl_xor_sync(hmask, pr, o));
+        pr = __reduce_min_sync(hmask, (i < hdr_nt(h)) ? T.pr : MF_P8);
     }
     if (cnt) {
         // the half-warp's own counter slots (lane 0 writes, no atomics): tile
         // products and entries of the executed precision; a half-warp's counts
         // stay far below 2^32 per solve
-        int sl = len;
-#pragma unroll
-        for (int o = 8; o; o >>= 1) sl += __shfl_xor_sync(hmask, sl, o);
+        const unsigned sl = __reduce_add_sync(hmask, (unsigned)len);
         if (i == 0) {
             cnt[pr] += (unsigned)hdr_nt(h);
-            cnt[5 + pr] += (unsigned)sl;
+            cnt[5 + pr] += sl;
         }
     }
     if (MODE == MODE_FP64 || F64) return slice_dot_uniform<MF_P64>(P, h, off, i, hmask, len, T, X, pre);
@@ -438,8 +434,7 @@ __device__ __forceinline__ void spmv_range_f32(const SolverParams &P, int sb, in
         len = lenn;
     }
     if (cnt) {
-#pragma unroll
-        for (int o = 8; o; o >>= 1) nent += __shfl_xor_sync(hmask, nent, o);
+        nent = __reduce_add_sync(hmask, nent);
         if (i == 0) {
             cnt[MF_P32] += ntiles;
             cnt[5 + MF_P32] += nent;
@@ -535,18 +530,16 @@ __device__ __forceinline__ Ctx make_ctx(const SolverParams &P)
 }
 
 // max over the 16 lanes of a half-warp; hmask names exactly those lanes (the
-// two halves of a warp walk different tile-row ranges, so they never shuffle together)
+// two halves of a warp walk different tile-row ranges, so they never reduce
+// together).  One redux.sync instead of a shuffle tree.  half_max takes
+// magnitudes (v >= 0), whose IEEE order is the order of their bit patterns.
 __device__ __forceinline__ float half_max(float v, unsigned hmask)
 {
-#pragma unroll
-    for (int o = 8; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(hmask, v, o));
-    return v;
+    return __int_as_float(__reduce_max_sync(hmask, __float_as_int(v)));
 }
 __device__ __forceinline__ int half_max_i(int v, unsigned hmask)
 {
-#pragma unroll
-    for (int o = 8; o; o >>= 1) v = max(v, __shfl_xor_sync(hmask, v, o));
-    return v;
+    return __reduce_max_sync(hmask, v);
 }
 
 // reference label rank of |dp| (main-cg-mixed.cu:1334-1351): 4 FP64, 3 FP32, 2 FP16, 1 INT8, 0 none
@@ -1306,9 +1299,7 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
             pr = MF_P32;                 // no tile can leave FP32 in this SpMV: no lookups
         } else if (kMixed) {
             const float st = (i < hdr_nt(h)) ? mag[tw >> 8] : 0.0f;
-            pr = (i < hdr_nt(h)) ? tile_prec<MODE, false>(P, tw, st, X) : MF_P8;
-#pragma unroll
-            for (int o = 8; o; o >>= 1) pr = min(pr, __shfl_xor_sync(hmask, pr, o));
+            pr = __reduce_min_sync(hmask, (i < hdr_nt(h)) ? tile_prec<MODE, false>(P, tw, st, X) : MF_P8);
         }
         float sc = 0.0f;
         if (kMixed && pr == MF_P8) sc = (i < hdr_nt(h)) ? P.i8_scale[h.x + i] : 0.0f;
