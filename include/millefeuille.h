@@ -128,6 +128,11 @@ typedef struct {
     int test_stall_barrier;/* test hook: 1 = the first grid barrier waits for one arrival that
                               never comes; the bounded wait runs out after wait_timeout_s and the
                               solve returns MF_ERR_TIMEOUT (no fault, the context stays usable) */
+    double demote_min_fraction; /* mixed: narrower tiles are considered in an SpMV only when at least
+                              this fraction of the operand's column segments fell below demote_fp16
+                              of its maximum in the previous update (or of the tiles are exact in a
+                              narrower type, for use_lossless); below it every tile runs FP32.
+                              Default 0.125; 0 = always consider them */
 } mf_options;
 
 typedef struct {

@@ -62,6 +62,7 @@ void mf_options_default(mf_options *o)
     o->x0_given = 0;
     o->l2_window = 1;
     o->test_stall_barrier = 0;
+    o->demote_min_fraction = 0.125;
 }
 
 void mf_free_host(void *p) { free(p); }

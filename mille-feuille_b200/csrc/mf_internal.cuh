@@ -88,6 +88,9 @@ struct mf_matrix_s {
     // cached solver workspace
     void *ws;
     size_t ws_bytes;
+    // tiles exact in INT8 or FP16 (counted on first use; n_exact_known = 0 before)
+    int n_exact_known;
+    long long n_exact;
 };
 
 // ---------------------------------------------------------------- helpers

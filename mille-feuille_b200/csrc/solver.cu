@@ -65,7 +65,9 @@ struct SolverParams {
     unsigned long long *counts;
     unsigned long long *phase_ns;   // [8] block-0 time per phase: spmv, vecB, vecC, barrier, replacement
     int method, max_iter, fixed_iters, replace_every, use_lossless;
-    int lossless_any;             // use_lossless and some tile is exact in INT8 / FP16
+    int lossless_any;             // use_lossless and enough tiles are exact in INT8 / FP16
+    float min_small;              // mixed: narrower tiles only when at least this many column
+                                  // segments were small in the operand's previous update
     double tol;
     float demote16, demote8;
     unsigned long long timeout_ns;
@@ -573,13 +575,16 @@ __device__ __forceinline__ int8_t trunc_i8(double v)
 template <int MODE>
 __device__ __forceinline__ void publish_dir(int R, int row, bool valid, double vnew, double vold, float *v32,
                                             __half *v16, int8_t *v8, float *mag, signed char *lab, float &bmax,
-                                            unsigned hmask, bool labels, float *bmin = nullptr)
+                                            unsigned hmask, bool labels, float *bmin = nullptr,
+                                            float small_thr = -1.0f, float *nsmall = nullptr)
 {
     if (MODE == MODE_PARITY && valid) v32[row] = (float)vnew;
     if (MODE == MODE_MIXED) {
         float m = half_max(valid ? (float)fabs(vnew) : 0.0f, hmask);
         bmax = fmaxf(bmax, m);
         if (bmin) *bmin = fminf(*bmin, m);
+        // segments at or below small_thr (demote_fp16 x the operand's previous maximum)
+        if (nsmall && (threadIdx.x & 15) == 0 && m <= small_thr) *nsmall += 1.0f;
         if ((threadIdx.x & 15) == 0) mag[R] = m;
     } else if (MODE == MODE_PARITY) {
         if (valid) {
@@ -675,7 +680,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
 
     // ---- init: x = 0 (owned rows), r = b, p = r (rh = r) ----
     double pb = 0.0;
-    float bmax = 0.0f, bmin = 3.0e38f;
+    float bmax = 0.0f, bmin = 3.0e38f, nsm = 0.0f;   // no previous maximum: nothing counts as small
     for (int R = c.rbeg; R < c.rend; R++) {
         const int row = R * MF_BS + c.i;
         const bool valid = row < n;
@@ -692,18 +697,24 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     }
     // the smallest segment magnitude (carried as -min) matters only to the mixed
     // mode's SpMV; FP64 and parity reduce (sum, max) as before
-    constexpr int kNvSeg = (MODE == MODE_MIXED) ? 3 : 2;
-    block_partial(P, sh, 0, pb, (double)bmax, -(double)bmin, 0, kNvSeg, 0x6u);
+    // (sum, max, -min, small segments) in mixed mode; FP64 and parity reduce (sum, max)
+    constexpr int kNvSeg = (MODE == MODE_MIXED) ? 4 : 2;
+    constexpr int kNvSegB = (MODE == MODE_MIXED) ? 3 : 1;      // (max, -min, small) without a sum
+    block_partial(P, sh, 0, pb, (double)bmax, -(double)bmin, (double)nsm, kNvSeg, 0x6u);
     if (!grid_barrier(P, epoch, sh)) return;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     grid_collect(P, sh, 0, kNvSeg, 0x6u, v);
     // mixed: can any tile of the next SpMV leave FP32 at all?  Not when the
     // smallest column segment is within demote_fp16 of the largest and no tile
     // is exact in a narrower type: then the SpMV skips its precision lookups.
-    auto dyn_of = [&](double mx, double neg_mn) -> int {
-        return (P.lossless_any || mx <= 0.0 || -neg_mn <= (double)P.demote16 * mx) ? 1 : 0;
+    // And narrower tiles are considered only when enough segments were small
+    // (demote_min_fraction): a few demoted tiles save fewer bytes than the
+    // lookups cost in a latency-bound SpMV.
+    auto dyn_of = [&](double mx, double neg_mn, double nsmall) -> int {
+        return (P.lossless_any ||
+                ((mx <= 0.0 || -neg_mn <= (double)P.demote16 * mx) && nsmall >= (double)P.min_small)) ? 1 : 0;
     };
-    int dynA = (MODE == MODE_MIXED) ? dyn_of(v[1], v[2]) : 0;
+    int dynA = (MODE == MODE_MIXED) ? dyn_of(v[1], v[2], v[3]) : 0;
             clk.lap(PH_BAR);
     const double bb = v[0];
     double rr = v[0], r1 = v[0];
@@ -763,7 +774,8 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             if (!isfinite(alpha2)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B: x += alpha p; r -= alpha q; r.r; r's shadow ----
             double prr = 0.0;
-            float rmax = 0.0f, rmin = 3.0e38f;
+            float rmax = 0.0f, rmin = 3.0e38f, rsm = 0.0f;
+            const float rthr = invM > 0.0f ? P.demote16 / invM : -1.0f;
             // kVB tile-rows per step: all loads first, so kVB round trips overlap
             for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
                 double xv[kVB], pv[kVB], rv[kVB], qv[kVB];
@@ -789,18 +801,18 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                         prr += rn * rn;
                     }
                     publish_dir<MODE>(R, row, valid, rn, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
-                                      c.hmask, false, &rmin);
+                                      c.hmask, false, &rmin, rthr, &rsm);
                 }
             }
             clk.lap(PH_VECB);
-            block_partial(P, sh, 2, prr, (double)rmax, -(double)rmin, 0, kNvSeg, 0x6u);
+            block_partial(P, sh, 2, prr, (double)rmax, -(double)rmin, (double)rsm, kNvSeg, 0x6u);
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 2, kNvSeg, 0x6u, v);
             clk.lap(PH_BAR);
             double rr_new = v[0];
             const double rr_rec = rr_new;       // recursive r.r of this iteration
             invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
-            if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2]);
+            if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2], v[3]);
             k++;
             last_true = 0;
             const bool want_check = !P.fixed_iters && rr_new <= thr2;
@@ -811,6 +823,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 double prt = 0.0;
                 rmax = 0.0f;
                 rmin = 3.0e38f;
+                rsm = 0.0f;
                 spmv_range<MODE, true>(P, c.sbeg, c.send, c.i, c.hmask, fp64_x(P.x), nullptr,
                                        [&](int R, double y) {
                                            const int row = R * MF_BS + c.i;
@@ -822,7 +835,8 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                                                prt += rv * rv;
                                            }
                                            publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr,
-                                                             P.mag_r, nullptr, rmax, c.hmask, false, &rmin);
+                                                             P.mag_r, nullptr, rmax, c.hmask, false, &rmin,
+                                                             rthr, &rsm);
                                        });
                 if (has_empty) {
                     for (int R = c.rbeg; R < c.rend; R++) {
@@ -835,17 +849,17 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                             prt += rv * rv;
                         }
                         publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
-                                          c.hmask, false, &rmin);
+                                          c.hmask, false, &rmin, rthr, &rsm);
                     }
                 }
                 clk.lap(PH_REPL);
-                block_partial(P, sh, 5, prt, (double)rmax, -(double)rmin, 0, kNvSeg, 0x6u);
+                block_partial(P, sh, 5, prt, (double)rmax, -(double)rmin, (double)rsm, kNvSeg, 0x6u);
                 if (!grid_barrier(P, epoch, sh)) return;
                 grid_collect(P, sh, 5, kNvSeg, 0x6u, v);
                 clk.lap(PH_BAR);
                 rr_new = v[0];
                 invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
-                if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2]);
+                if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2], v[3]);
                 rr_true = rr_new;
                 repl++;
                 last_true = 1;
@@ -924,7 +938,8 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             alpha = r1 / v[0];
             if (!isfinite(alpha)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B1: s = r - alpha v ----
-            float smax = 0.0f, smin = 3.0e38f;
+            float smax = 0.0f, smin = 3.0e38f, ssm = 0.0f;
+            const float sthr = invMs > 0.0f ? P.demote16 / invMs : -1.0f;
             for (int R = c.rbeg; R < c.rend; R++) {
                 const int row = R * MF_BS + c.i;
                 const bool valid = row < n;
@@ -935,16 +950,16 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                     P.s[row] = sn;
                 }
                 publish_dir<MODE>(R, row, valid, sn, sold, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, smax, c.hmask,
-                                  true, &smin);
+                                  true, &smin, sthr, &ssm);
             }
             clk.lap(PH_VECB);
             // (max, -min) of s's segment magnitudes; only the mixed mode uses the minimum
-            block_partial(P, sh, 2, (double)smax, -(double)smin, 0, 0, kNvSeg - 1, 0x3u);
+            block_partial(P, sh, 2, (double)smax, -(double)smin, (double)ssm, 0, kNvSegB, 0x3u);
             if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 2, kNvSeg - 1, 0x3u, v);
+            grid_collect(P, sh, 2, kNvSegB, 0x3u, v);
             clk.lap(PH_BAR);
             invMs = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
-            const int dynS = (MODE == MODE_MIXED) ? dyn_of(v[0], v[1]) : 1;
+            const int dynS = (MODE == MODE_MIXED) ? dyn_of(v[0], v[1], v[2]) : 1;
             // ---- A2: t = A s, omega = (t.s)/(t.t) ----
             double pts = 0.0, ptt = 0.0;
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
@@ -1053,7 +1068,8 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
         }
         rr = rr_new;
         bmax = 0.0f;
-        float pmin = 3.0e38f;
+        float pmin = 3.0e38f, psm = 0.0f;
+        const float pthr = invM > 0.0f ? P.demote16 / invM : -1.0f;
         for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
             double pv[kVB], rv[kVB], xq[kVB];    // xq: x (CG, x not yet updated) or v (BiCGSTAB)
 #pragma unroll
@@ -1078,16 +1094,16 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                     if (bicg && restart) P.rh[row] = rv[u];
                 }
                 publish_dir<MODE>(R, row, valid, valid ? pn : 0.0, pold, P.p32, P.p16, P.p8, P.mag_p, P.lab_p,
-                                  bmax, c.hmask, true, &pmin);
+                                  bmax, c.hmask, true, &pmin, pthr, &psm);
             }
         }
         clk.lap(PH_VECC);
-        block_partial(P, sh, 6, (double)bmax, -(double)pmin, 0, 0, kNvSeg - 1, 0x3u);
+        block_partial(P, sh, 6, (double)bmax, -(double)pmin, (double)psm, 0, kNvSegB, 0x3u);
         if (!grid_barrier(P, epoch, sh)) return;
-        grid_collect(P, sh, 6, kNvSeg - 1, 0x3u, v);
+        grid_collect(P, sh, 6, kNvSegB, 0x3u, v);
             clk.lap(PH_BAR);
         invM = v[0] > 0.0 ? (float)(1.0 / v[0]) : 0.0f;
-        if (MODE == MODE_MIXED) dynA = dyn_of(v[0], v[1]);
+        if (MODE == MODE_MIXED) dynA = dyn_of(v[0], v[1], v[2]);
     }
     // ---- final FP64 true residual when the last one was not already formed ----
     if (!last_true) {
@@ -1748,7 +1764,9 @@ struct BatchItem {
     MultiParams M;                // the item's interleaved vectors and report words (M.nr columns used);
                                   // team items: M.red holds the team's partials [kinds][team][kRedWidthM]
     unsigned *ctr;                // team items: the team's barrier counter (zeroed before the launch)
+    long long n_exact;            // tiles exact in INT8 / FP16
     int n, tilem, nr;             // nr: interleave width (1, 2, 4 or 8)
+    int tilenum;
     int team;                     // blocks solving the item (1: queue item)
 };
 
@@ -1763,7 +1781,7 @@ struct BatchParams {
     unsigned long long timeout_ns, arrive_timeout_ns;
     int stall_first;              // test hook: a team's first barrier expects one extra arrival
     int max_iter, fixed_iters, replace_every, use_lossless;
-    double tol;
+    double tol, min_fraction;
     float demote16, demote8;
 };
 
@@ -1925,7 +1943,8 @@ __device__ __forceinline__ SolverParams item_params(const BatchItem &it, const B
     P.fixed_iters = B.fixed_iters;
     P.replace_every = B.replace_every;
     P.use_lossless = B.use_lossless;
-    P.lossless_any = B.use_lossless;     // conservative: the batch does not scan its tiles
+    P.lossless_any = (B.use_lossless && it.n_exact > 0 && (double)it.n_exact >= B.min_fraction * (double)it.tilenum)
+                         ? 1 : 0;
     P.tol = B.tol;
     P.demote16 = B.demote16;
     P.demote8 = B.demote8;
@@ -2022,7 +2041,6 @@ struct Workspace {
     int *hw_begin;
     int nhw;
     cudaEvent_t e0, e1;
-    int any_exact;         // some tile is exact in INT8 or FP16 (lossless classes can apply)
     // several right-hand sides (k_solve_multi): interleaved vectors for NR columns
     int m_nr, m_G;
     double *m_vec;         // B | X | R | P | Q, each vec_len * NR
@@ -2044,13 +2062,37 @@ int dal(T **p, long long count)
         if (_rc != MF_SUCCESS) return _rc;  \
     } while (0)
 
-__global__ void k_any_exact(const unsigned char *caps, int n, int *flag)
+__global__ void k_count_exact(const unsigned char *caps, int n, unsigned long long *count)
 {
+    unsigned c = 0;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        if (caps[t] & (MF_CAP_EXACT_I8 | MF_CAP_EXACT_F16)) {
-            atomicOr(flag, 1);
-            return;
-        }
+        if (caps[t] & (MF_CAP_EXACT_I8 | MF_CAP_EXACT_F16)) c++;
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// Tiles exact in INT8 or FP16 (the lossless classes), counted once per matrix
+// through `scratch` (one unsigned long long of device memory).
+int exact_tiles(mf_matrix_s *A, unsigned long long *scratch, cudaStream_t s)
+{
+    if (!A->n_exact_known) {
+        unsigned long long h = 0;
+        MF_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(h), s));
+        if (A->tilenum > 0) k_count_exact<<<256, 256, 0, s>>>(A->d_tile_caps, A->tilenum, scratch);
+        MF_CUDA_TRY(cudaGetLastError());
+        MF_CUDA_TRY(cudaMemcpyAsync(&h, scratch, sizeof(h), cudaMemcpyDeviceToHost, s));
+        MF_CUDA_TRY(cudaStreamSynchronize(s));
+        A->n_exact = (long long)h;
+        A->n_exact_known = 1;
+    }
+    return MF_SUCCESS;
+}
+
+// Lossless classes apply when asked for and enough tiles are exact in a narrower
+// type (the same fraction that gates demotion by magnitude).
+inline int lossless_on(int use_lossless, double min_fraction, long long n_exact, int tilenum)
+{
+    return (use_lossless && n_exact > 0 && (double)n_exact >= min_fraction * (double)tilenum) ? 1 : 0;
 }
 
 const void *solve_kernel(int mode, int lb)
@@ -2127,14 +2169,7 @@ int ws_get(mf_matrix_s *A, int blocks_per_sm, Workspace **out, cudaStream_t s)
     MF_TRY(dal(&w->bar, 1)); MF_TRY(dal(&w->err, 1)); MF_TRY(dal(&w->out, 16));
     MF_TRY(dal(&w->counts, 16));
     MF_TRY(dal(&w->phase_ns, 8));
-    {
-        int *flag = (int *)w->counts;       // scratch before the first solve zeroes it
-        MF_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(int), s));
-        if (A->tilenum > 0) k_any_exact<<<256, 256, 0, s>>>(A->d_tile_caps, A->tilenum, flag);
-        MF_CUDA_TRY(cudaGetLastError());
-        MF_CUDA_TRY(cudaMemcpyAsync(&w->any_exact, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MF_CUDA_TRY(cudaStreamSynchronize(s));
-    }
+    MF_TRY(exact_tiles(A, w->counts, s));    // counts: scratch before the first solve zeroes it
     w->nhw = G * kWarps * 2;
     MF_TRY(dal(&w->hw_begin, w->nhw + 1));
     MF_CUDA_TRY(cudaEventCreate(&w->e0));
@@ -2287,7 +2322,8 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     P.fixed_iters = opt->fixed_iters;
     P.replace_every = opt->replace_every;
     P.use_lossless = opt->use_lossless;
-    P.lossless_any = (opt->use_lossless && w->any_exact) ? 1 : 0;
+    P.lossless_any = lossless_on(opt->use_lossless, opt->demote_min_fraction, A->n_exact, A->tilenum);
+    P.min_small = (float)(opt->demote_min_fraction * (double)A->tilem);
     P.tol = opt->tol;
     P.demote16 = (float)opt->demote_fp16;
     P.demote8 = (float)opt->demote_int8;
@@ -2551,7 +2587,8 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
     P.fixed_iters = opt->fixed_iters;
     P.replace_every = opt->replace_every;
     P.use_lossless = opt->use_lossless;
-    P.lossless_any = (opt->use_lossless && w->any_exact) ? 1 : 0;
+    P.lossless_any = lossless_on(opt->use_lossless, opt->demote_min_fraction, A->n_exact, A->tilenum);
+    P.min_small = (float)(opt->demote_min_fraction * (double)A->tilem);
     P.tol = opt->tol;
     P.demote16 = (float)opt->demote_fp16;
     P.demote8 = (float)opt->demote_int8;
@@ -2729,6 +2766,16 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
             B.it_nr.push_back(mf_batch_width(g));
         }
     B.nitems = (int)B.it_sys.size();
+    {
+        // exact-tile counts of the systems (once per matrix)
+        unsigned long long *scratch = nullptr;
+        MF_CUDA_TRY(cudaMalloc((void **)&scratch, sizeof(*scratch)));
+        int rc = MF_SUCCESS;
+        for (mf_matrix_s *A : B.sys)
+            if (rc == MF_SUCCESS) rc = exact_tiles(A, scratch, s);
+        cudaFree(scratch);
+        MF_TRY(rc);
+    }
     std::vector<double> cost(B.nitems);
     std::vector<int> tilem(B.nitems);
     for (int t = 0; t < B.nitems; t++) {
@@ -2784,6 +2831,7 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
         it.seg_rowlen = A->d_seg_rowlen; it.meta = A->d_meta; it.v64 = A->d_v64; it.v32 = A->d_v32;
         it.v16 = A->d_v16; it.v8 = A->d_v8; it.i8_scale = A->d_i8_scale; it.row_cost = A->d_row_cost;
         it.n = A->n_rows; it.tilem = A->tilem; it.nr = (int)nr; it.team = B.it_team[t];
+        it.n_exact = A->n_exact; it.tilenum = A->tilenum;
         char *base = B.d_pool + off[t];
         double *v = (double *)base;
         it.M.B = v; it.M.X = v + L * nr; it.M.R = v + 2 * L * nr; it.M.Pv = v + 3 * L * nr; it.M.Q = v + 4 * L * nr;
@@ -2928,6 +2976,7 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
     bp.replace_every = opt->replace_every;
     bp.use_lossless = opt->use_lossless;
     bp.tol = opt->tol;
+    bp.min_fraction = opt->demote_min_fraction;
     bp.demote16 = (float)opt->demote_fp16;
     bp.demote8 = (float)opt->demote_int8;
     // team waits: within an item the members run in step (the normal bound);
@@ -2957,7 +3006,7 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
         }
         const double opts[] = {opt->tol, (double)opt->max_iter, (double)opt->fixed_iters, (double)opt->replace_every,
                                opt->demote_fp16, opt->demote_int8, (double)opt->use_lossless, (double)B.cap,
-                               opt->wait_timeout_s, (double)opt->test_stall_barrier};
+                               opt->wait_timeout_s, (double)opt->test_stall_barrier, opt->demote_min_fraction};
         for (double v : opts) {
             unsigned long long u;
             memcpy(&u, &v, sizeof(u));

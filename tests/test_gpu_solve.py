@@ -101,6 +101,10 @@ def test_gpu_mixed_demotes_small_segments_and_converges(mf, cuda, p3d):
     x, rep = G.solve(b, method="cg", precision="mixed", tol=1e-8)
     assert rep["converged"] and _relres(A, x, b) <= 1.0001e-8
     assert rep["tile_uses"][2] + rep["tile_uses"][3] > 0, rep["tile_uses"]
+    # demote_min_fraction = 1: narrower tiles only if every segment is small -> all FP32
+    x1, rep1 = G.solve(b, method="cg", precision="mixed", tol=1e-8, demote_min_fraction=1.0)
+    assert rep1["converged"] and _relres(A, x1, b) <= 1.0001e-8
+    assert rep1["tile_uses"][2] + rep1["tile_uses"][3] == 0 and rep1["tile_uses"][1] > 0, rep1["tile_uses"]
     X, reps = G.solve_multi(np.stack([b, b[::-1].copy()]), method="cg", precision="mixed", tol=1e-8)
     for k in range(2):
         assert reps[k]["converged"] and _relres(A, X[k], [b, b[::-1]][k]) <= 1.0001e-8
