@@ -1217,7 +1217,6 @@ struct SharedM {
 struct MultiParams {
     const double *B;          // [vec_len * NR] interleaved right-hand sides (zero columns past nr)
     double *X, *R, *Pv, *Q;   // interleaved
-    float *R32;               // interleaved FP32 shadow of R (mixed)
     float *mag;               // per tile-row: max over its rows and columns of |R|
     double *red;              // [kinds][G][kRedWidthM]
     double *out;              // per column: iterations, converged, true rel. residual, recursive; then k, status
@@ -1288,11 +1287,11 @@ __device__ void grid_collect_m(const MultiParams &M, SharedM &sh, int kind, unsi
 // slice_dot (mixed: from the column segments' max over rows and columns).
 template <int MODE, int NR, bool F64, typename Epi>
 __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se, int i, unsigned hmask,
-                                           const double *X64, const float *X32, const float *mag, float invM,
+                                           const double *X64, const float *mag, float invM,
                                            int dyn, Epi epi)
 {
     constexpr bool kMixed = (MODE == MODE_MIXED) && !F64;
-    XVec X = make_x(X64, X32, nullptr, nullptr, mag, nullptr, invM, dyn);
+    XVec X = make_x(X64, nullptr, nullptr, nullptr, mag, nullptr, invM, dyn);
     double acc[NR];
 #pragma unroll
     for (int k = 0; k < NR; k++) acc[k] = 0.0;
@@ -1345,9 +1344,8 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
                     }
                 }
             } else {
-                float part[NR];
-#pragma unroll
-                for (int k = 0; k < NR; k++) part[k] = 0.0f;
+                // stored FP32 / FP16 / scaled-INT8 values widened to FP64 against the
+                // FP64 operand rows (as the single-column walk): no FP32 copy of R
 #pragma unroll
                 for (int j = 0; j < 8; j++) {
                     const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
@@ -1356,24 +1354,22 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
                     const float s8 = (pr == MF_P8) ? __shfl_sync(hmask, sc, slot, 16) : 0.0f;
                     if (k0 + j < len) {
                         const long long e = off + (long long)(k0 + j) * MF_BS + i;
-                        const float v = (pr == MF_P32)   ? __ldcs(P.v32 + e)
-                                        : (pr == MF_P16) ? __half2float(P.v16[e])
-                                                         : (float)P.v8[e] * s8;
+                        const double v = (pr == MF_P32)   ? (double)__ldcs(P.v32 + e)
+                                         : (pr == MF_P16) ? (double)__half2float(P.v16[e])
+                                                          : (double)((float)P.v8[e] * s8);
                         if constexpr (NR == 1) {
-                            part[0] = fmaf(v, X32[xi], part[0]);
+                            acc[0] = fma(v, X64[xi], acc[0]);
                         } else {
-                            const float2 *xr = (const float2 *)(X32 + (long long)xi * NR);
+                            const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
 #pragma unroll
                             for (int q = 0; q < NR / 2; q++) {
-                                const float2 d = xr[q];
-                                part[2 * q] = fmaf(v, d.x, part[2 * q]);
-                                part[2 * q + 1] = fmaf(v, d.y, part[2 * q + 1]);
+                                const double2 d = xr[q];
+                                acc[2 * q] = fma(v, d.x, acc[2 * q]);
+                                acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
                             }
                         }
                     }
                 }
-#pragma unroll
-                for (int k = 0; k < NR; k++) acc[k] += (double)part[k];
             }
         }
         if (hdr_last(h)) {
@@ -1392,8 +1388,8 @@ struct SegMM {
     float mx, mn;
 };
 
-// R's FP32 shadow and segment magnitude (max over the tile-row's rows and all
-// columns) for tile-row R; all 16 lanes of the half-warp call it together.
+// R's segment magnitude (max over the tile-row's rows and all columns) for
+// tile-row R; all 16 lanes of the half-warp call it together.
 template <int MODE, int NR>
 __device__ __forceinline__ void publish_multi(const MultiParams &M, int R, int row, bool valid, const double (&rv)[NR],
                                               SegMM &st, unsigned hmask)
@@ -1401,17 +1397,8 @@ __device__ __forceinline__ void publish_multi(const MultiParams &M, int R, int r
     if (MODE != MODE_MIXED) return;
     float m = 0.0f;
     if (valid) {
-        if constexpr (NR == 1) {
-            M.R32[row] = (float)rv[0];
-            m = fabsf((float)rv[0]);
-        } else {
-            float2 *dst = (float2 *)(M.R32 + (long long)row * NR);
 #pragma unroll
-            for (int q = 0; q < NR / 2; q++) {
-                dst[q] = make_float2((float)rv[2 * q], (float)rv[2 * q + 1]);
-                m = fmaxf(m, fmaxf(fabsf((float)rv[2 * q]), fabsf((float)rv[2 * q + 1])));
-            }
-        }
+        for (int q = 0; q < NR; q++) m = fmaxf(m, fabsf((float)rv[q]));
     }
     m = half_max(m, hmask);
     st.mx = fmaxf(st.mx, m);
@@ -1534,7 +1521,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
                 store_row<NR>(M.Q, row, q);
             }
         };
-        spmv_multi<MODE, NR, false>(P, c.sbeg, c.send, c.i, c.hmask, M.R, M.R32, M.mag, invM, dyn, upd_a);
+        spmv_multi<MODE, NR, false>(P, c.sbeg, c.send, c.i, c.hmask, M.R, M.mag, invM, dyn, upd_a);
         if (has_empty) {
             double zw[NR];
 #pragma unroll
@@ -1622,7 +1609,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
                 }
                 publish_multi<MODE, NR>(M, R, row, valid, r, st, c.hmask);
             };
-            spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, 1, upd_r);
+            spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, 0.0f, 1, upd_r);
             if (has_empty) {
                 double zy[NR];
 #pragma unroll
@@ -1672,7 +1659,7 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
                 for (int j = 0; j < NR; j++) prt[j] += (b[j] - y[j]) * (b[j] - y[j]);
             }
         };
-        spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, nullptr, 0.0f, 1, acc_r);
+        spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, 0.0f, 1, acc_r);
         if (has_empty) {
             double zy[NR];
 #pragma unroll
@@ -2044,7 +2031,7 @@ struct Workspace {
     // several right-hand sides (k_solve_multi): interleaved vectors for NR columns
     int m_nr, m_G;
     double *m_vec;         // B | X | R | P | Q, each vec_len * NR
-    float *m_r32, *m_mag;
+    float *m_mag;
     double *m_red, *m_out;
     int *m_hw_begin;
 };
@@ -2271,7 +2258,7 @@ void mf_solver_free_ws(mf_matrix_s *A)
     Workspace *w = (Workspace *)A->ws;
     if (!w) return;
     void *ptrs[] = {w->vecs, w->mag_p, w->mag_s, w->lab_p, w->lab_s, w->red, w->bar, w->err, w->out, w->counts,
-                    w->phase_ns, w->hw_begin, w->m_vec, w->m_r32, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
+                    w->phase_ns, w->hw_begin, w->m_vec, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     cudaEventDestroy(w->e0);
@@ -2529,10 +2516,10 @@ const void *multi_kernel(int mode, int nr)
 int ws_multi(mf_matrix_s *A, Workspace *w, int mode, int nr, cudaStream_t s)
 {
     if (w->m_nr == nr && w->m_vec) return MF_SUCCESS;
-    void *old[] = {w->m_vec, w->m_r32, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
+    void *old[] = {w->m_vec, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
     for (void *p : old)
         if (p) cudaFree(p);
-    w->m_vec = nullptr; w->m_r32 = nullptr; w->m_mag = nullptr; w->m_red = nullptr; w->m_out = nullptr;
+    w->m_vec = nullptr; w->m_mag = nullptr; w->m_red = nullptr; w->m_out = nullptr;
     w->m_hw_begin = nullptr;
     w->m_nr = 0;
     int dev = 0, nsm = 0, occ = 0;
@@ -2549,13 +2536,11 @@ int ws_multi(mf_matrix_s *A, Workspace *w, int mode, int nr, cudaStream_t s)
     if (need < G) G = need > 0 ? need : 1;
     const long long L = A->vec_len, S = std::max(A->tilem, A->tilen) + 1;
     MF_TRY(dal(&w->m_vec, 5 * L * nr));
-    MF_TRY(dal(&w->m_r32, L * nr));
     MF_TRY(dal(&w->m_mag, S));
     MF_TRY(dal(&w->m_red, (long long)kRedKinds * G * kRedWidthM));
     MF_TRY(dal(&w->m_out, 4 * kMaxNR + 8));
     MF_TRY(dal(&w->m_hw_begin, (long long)G * kWarps * 2 + 1));
     MF_CUDA_TRY(cudaMemsetAsync(w->m_vec, 0, (size_t)5 * L * nr * sizeof(double), s));
-    MF_CUDA_TRY(cudaMemsetAsync(w->m_r32, 0, (size_t)L * nr * sizeof(float), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->m_mag, 0, (size_t)S * sizeof(float), s));
     const int nhw = G * kWarps * 2;
     k_partition<<<(nhw + 256) / 256, 256, 0, s>>>(A->d_row_cost, A->tilem, nhw, w->m_hw_begin);
@@ -2601,7 +2586,6 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
     M.R = w->m_vec + 2 * L * nr;
     M.Pv = w->m_vec + 3 * L * nr;
     M.Q = w->m_vec + 4 * L * nr;
-    M.R32 = w->m_r32;
     M.mag = w->m_mag;
     M.red = w->m_red;
     M.out = w->m_out;
@@ -2794,7 +2778,7 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
         bptr.assign(B.grid + 1, 0);
     }
     B.nqueue = (int)queue.size();
-    // per item: B | X | R | P | Q (doubles), R32 (floats), segment magnitudes,
+    // per item: B | X | R | P | Q (doubles), segment magnitudes,
     // report words, team partials
     std::vector<size_t> off(B.nitems), red_off(B.nitems, 0);
     size_t total = 0;
@@ -2803,8 +2787,7 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
         const mf_matrix_s *A = B.sys[B.it_sys[t]];
         const size_t L = (size_t)A->vec_len, nr = (size_t)B.it_nr[t];
         off[t] = total;
-        total += align256(5 * L * nr * sizeof(double)) + align256(L * nr * sizeof(float)) +
-                 align256((size_t)(A->tilem + 1) * sizeof(float));
+        total += align256(5 * L * nr * sizeof(double)) + align256((size_t)(A->tilem + 1) * sizeof(float));
         B.out_off[t] = total;
         total += align256(kOutWords * sizeof(double));
         if (B.it_team[t] > 1) {
@@ -2835,9 +2818,7 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
         char *base = B.d_pool + off[t];
         double *v = (double *)base;
         it.M.B = v; it.M.X = v + L * nr; it.M.R = v + 2 * L * nr; it.M.Pv = v + 3 * L * nr; it.M.Q = v + 4 * L * nr;
-        char *f = base + align256(5 * L * nr * sizeof(double));
-        it.M.R32 = (float *)f;
-        it.M.mag = (float *)(f + align256(L * nr * sizeof(float)));
+        it.M.mag = (float *)(base + align256(5 * L * nr * sizeof(double)));
         it.M.red = it.team > 1 ? (double *)(B.d_pool + red_off[t]) : nullptr;
         it.M.out = (double *)(B.d_pool + B.out_off[t]);
         it.M.nr = B.it_ncol[t];
