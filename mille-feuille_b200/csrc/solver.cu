@@ -54,7 +54,7 @@ struct SolverParams {
     const double *b;
     double *x, *r, *p, *q, *rh, *s, *t;
     float *p32, *s32, *mag_p, *mag_s;
-    float *r32, *mag_r;           // CG with the SpMV on r: r's FP32 shadow / segment magnitudes
+    float *mag_r;                 // CG with the SpMV on r: r's segment magnitudes
     __half *p16, *s16;
     int8_t *p8, *s8;
     signed char *lab_p, *lab_s;
@@ -740,7 +740,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             // ---- A: w = A r; p = r + beta p; q = w + beta q; p.q ----
             double ppq = 0.0;
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
-                                    make_x(P.r, P.r32, nullptr, nullptr, P.mag_r, nullptr, invM, dynA), cnt,
+                                    make_x(P.r, nullptr, nullptr, nullptr, P.mag_r, nullptr, invM, dynA), cnt,
                                     [&](int R, double y) {
                                         const int row = R * MF_BS + c.i;
                                         if (row < n) {
@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                         P.r[row] = rn;
                         prr += rn * rn;
                     }
-                    publish_dir<MODE>(R, row, valid, rn, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
+                    publish_dir<MODE>(R, row, valid, rn, 0.0, nullptr, nullptr, nullptr, P.mag_r, nullptr, rmax,
                                       c.hmask, false, &rmin, rthr, &rsm);
                 }
             }
@@ -834,7 +834,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                                                P.r[row] = rv;
                                                prt += rv * rv;
                                            }
-                                           publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr,
+                                           publish_dir<MODE>(R, row, valid, rv, 0.0, nullptr, nullptr, nullptr,
                                                              P.mag_r, nullptr, rmax, c.hmask, false, &rmin,
                                                              rthr, &rsm);
                                        });
@@ -848,7 +848,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                             P.r[row] = rv;
                             prt += rv * rv;
                         }
-                        publish_dir<MODE>(R, row, valid, rv, 0.0, P.r32, nullptr, nullptr, P.mag_r, nullptr, rmax,
+                        publish_dir<MODE>(R, row, valid, rv, 0.0, nullptr, nullptr, nullptr, P.mag_r, nullptr, rmax,
                                           c.hmask, false, &rmin, rthr, &rsm);
                     }
                 }
@@ -2194,7 +2194,7 @@ void fill_params(SolverParams &P, mf_matrix_s *A, Workspace *w)
         P.p32 = w->p32; P.s32 = w->s32; P.p16 = w->p16; P.s16 = w->s16; P.p8 = w->p8; P.s8 = w->s8;
         P.mag_p = w->mag_p; P.mag_s = w->mag_s; P.lab_p = w->lab_p; P.lab_s = w->lab_s;
         // CG in the FP64 / mixed modes multiplies r, not p: r's shadow takes p's slots
-        P.r32 = w->p32; P.mag_r = w->mag_p;
+        P.mag_r = w->mag_p;
         P.red = w->red; P.bar = w->bar; P.err = w->err; P.out = w->out; P.counts = w->counts;
         P.phase_ns = w->phase_ns;
     }

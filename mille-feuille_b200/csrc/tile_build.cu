@@ -591,7 +591,6 @@ int mf_build_tiles(mf_matrix_s *A, cudaStream_t s)
     // scratch per warp: bitmap + prefix (span words each) + tile counters (<= 32 * span)
     long long words_per_warp = 2LL * span + 32LL * span;
     int global_mode = 0;
-    int warps_per_block = kWarps;
     size_t smem = 0;
     unsigned int *gscratch = nullptr;
     int tgrid = wgrid;
@@ -603,7 +602,6 @@ int mf_build_tiles(mf_matrix_s *A, cudaStream_t s)
         tgrid = 148 * 4;
         MF_TRY(dalloc(&gscratch, words_per_warp * (long long)tgrid * kWarps, s));
     }
-    (void)warps_per_block;
     if (smem > 48 * 1024) {
         MF_CUDA_TRY(cudaFuncSetAttribute(k_count_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         MF_CUDA_TRY(cudaFuncSetAttribute(k_fill_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
