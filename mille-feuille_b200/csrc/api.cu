@@ -294,6 +294,7 @@ extern "C" int mf_solve(mf_matrix A, const double *b, double *x, const mf_option
         MF_CUDA_TRY(cudaMemcpyAsync(tmp, b, nb, cudaMemcpyHostToDevice, s));
         db = tmp;
         dx = tmp + A->n_rows;
+        if (o.x0_given) MF_CUDA_TRY(cudaMemcpyAsync(dx, x, nb, cudaMemcpyHostToDevice, s));
     }
     int rc = mf_solver_run(A, db, dx, &o, report, s);
     if (!device_ptrs) {

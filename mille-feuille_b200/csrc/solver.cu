@@ -65,6 +65,7 @@ struct SolverParams {
     unsigned long long *counts;
     unsigned long long *phase_ns;   // [8] block-0 time per phase: spmv, vecB, vecC, barrier, replacement
     int method, max_iter, fixed_iters, replace_every, use_lossless;
+    int x0_given;                 // x holds the initial guess: r = b - A x at the start
     int lossless_any;             // use_lossless and enough tiles are exact in INT8 / FP16
     float min_small;              // mixed: narrower tiles only when at least this many column
                                   // segments were small in the operand's previous update
@@ -679,21 +680,54 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     const bool bicg = (P.method == MF_METHOD_BICGSTAB);
 
     // ---- init: x = 0 (owned rows), r = b, p = r (rh = r) ----
-    double pb = 0.0;
+    // With an initial guess: r = b - A x in FP64, and |b|^2 reduced on its own
+    // first (it scales the convergence test).
+    double pb = 0.0, bb0 = 0.0;
     float bmax = 0.0f, bmin = 3.0e38f, nsm = 0.0f;   // no previous maximum: nothing counts as small
-    for (int R = c.rbeg; R < c.rend; R++) {
-        const int row = R * MF_BS + c.i;
-        const bool valid = row < n;
-        const double bv = valid ? P.b[row] : 0.0;
-        if (valid) {
-            P.x[row] = 0.0;
-            P.r[row] = bv;
-            P.p[row] = bv;
-            if (bicg) P.rh[row] = bv;
+    if (P.x0_given) {
+        double pbb = 0.0;
+        for (int R = c.rbeg; R < c.rend; R++) {
+            const int row = R * MF_BS + c.i;
+            if (row < n) pbb += P.b[row] * P.b[row];
         }
-        // parity mode: labels start all FP64 (cudaMemset(d_vis, 0), main-cg-mixed.cu:2828)
-        publish_dir<MODE>(R, row, valid, bv, 0.0, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, false, &bmin);
-        pb += bv * bv;
+        block_partial(P, sh, 8, pbb, 0, 0, 0, 1, 0u);
+        if (!grid_barrier(P, epoch, sh)) return;
+        double vb[4] = {0.0, 0.0, 0.0, 0.0};
+        grid_collect(P, sh, 8, 1, 0u, vb);
+        bb0 = vb[0];
+        auto init_row = [&](int R, double y) {
+            const int row = R * MF_BS + c.i;
+            const bool valid = row < n;
+            const double rv = valid ? P.b[row] - y : 0.0;
+            if (valid) {
+                P.r[row] = rv;
+                P.p[row] = rv;
+                if (bicg) P.rh[row] = rv;
+            }
+            publish_dir<MODE>(R, row, valid, rv, 0.0, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, false,
+                              &bmin);
+            pb += rv * rv;
+        };
+        spmv_range<MODE, true>(P, c.sbeg, c.send, c.i, c.hmask, fp64_x(P.x), nullptr, init_row);
+        for (int R = c.rbeg; R < c.rend; R++)
+            if (P.seg_ptr[R] == P.seg_ptr[R + 1]) init_row(R, 0.0);
+        nspmv++;
+    } else {
+        for (int R = c.rbeg; R < c.rend; R++) {
+            const int row = R * MF_BS + c.i;
+            const bool valid = row < n;
+            const double bv = valid ? P.b[row] : 0.0;
+            if (valid) {
+                P.x[row] = 0.0;
+                P.r[row] = bv;
+                P.p[row] = bv;
+                if (bicg) P.rh[row] = bv;
+            }
+            // parity mode: labels start all FP64 (cudaMemset(d_vis, 0), main-cg-mixed.cu:2828)
+            publish_dir<MODE>(R, row, valid, bv, 0.0, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, bmax, c.hmask, false,
+                              &bmin);
+            pb += bv * bv;
+        }
     }
     // the smallest segment magnitude (carried as -min) matters only to the mixed
     // mode's SpMV; FP64 and parity reduce (sum, max) as before
@@ -716,7 +750,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     };
     int dynA = (MODE == MODE_MIXED) ? dyn_of(v[1], v[2], v[3]) : 0;
             clk.lap(PH_BAR);
-    const double bb = v[0];
+    const double bb = P.x0_given ? bb0 : v[0];
     double rr = v[0], r1 = v[0];
     float invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
     float invMs = 0.0f;
@@ -2273,13 +2307,14 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     const int mode = opt->precision == MF_PREC_FP64 ? MODE_FP64
                      : opt->precision == MF_PREC_PARITY ? MODE_PARITY : MODE_MIXED;
     if (opt->method != MF_METHOD_CG && opt->method != MF_METHOD_BICGSTAB) return MF_ERR_INVALID;
-    if (opt->x0_given) return MF_ERR_UNSUPPORTED;
     Workspace *w = nullptr;
     MF_TRY(ws_get(A, opt->blocks_per_sm, &w, s));
     const long long L = A->vec_len;
     const long long S = std::max(A->tilem, A->tilen) + 1;
     // zero the padded tails and the state the kernel reads before writing
     MF_CUDA_TRY(cudaMemsetAsync(w->x, 0, L * sizeof(double), s));
+    if (opt->x0_given)
+        MF_CUDA_TRY(cudaMemcpyAsync(w->x, d_x, (size_t)A->n_rows * sizeof(double), cudaMemcpyDeviceToDevice, s));
     MF_CUDA_TRY(cudaMemsetAsync(w->p, 0, L * sizeof(double), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->q, 0, L * sizeof(double), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->s, 0, L * sizeof(double), s));
@@ -2305,6 +2340,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     fill_params(P, A, w);
     P.b = d_b;
     P.method = opt->method;
+    P.x0_given = opt->x0_given ? 1 : 0;
     P.max_iter = opt->max_iter;
     P.fixed_iters = opt->fixed_iters;
     P.replace_every = opt->replace_every;

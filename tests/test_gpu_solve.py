@@ -244,3 +244,28 @@ def test_gpu_ragged_system_with_decoupled_rows(mf, oracle_mod, cuda, method, pre
         xo, ro = T.cg_fp64(b, tol=1e-10, max_iter=5000)
         np.testing.assert_allclose(x, xo, rtol=0, atol=1e-8 * np.abs(xo).max())
         assert abs(rep["iterations"] - ro["iterations"]) <= 0.05 * ro["iterations"] + 1
+
+
+@pytest.mark.parametrize("method,precision", [("cg", "fp64"), ("cg", "mixed"), ("bicgstab", "mixed")])
+def test_gpu_initial_guess(mf, cuda, p3d, cd3d, method, precision):
+    """x0_given: the solve starts from x (r = b - A x in FP64).  From the exact
+    solution it stops at once; restarted from a 1e-4 solution it reaches 1e-10
+    in fewer iterations than from zero, on host and on device buffers."""
+    import torch
+    A, b, _ = p3d if method == "cg" else cd3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    xc, rc = G.solve(b, method=method, precision=precision, tol=1e-10)
+    assert rc["converged"]
+    xs = __import__("scipy.sparse.linalg", fromlist=["spsolve"]).spsolve(A.to_scipy().tocsc(), b)
+    x0 = xs.copy()
+    x1, r1 = G.solve(b, x0, method=method, precision=precision, tol=1e-10, x0_given=1)
+    assert r1["converged"] and r1["iterations"] <= 1 and _relres(A, x1, b) <= 1e-10
+    xa, ra = G.solve(b, method=method, precision=precision, tol=1e-4)
+    xw, rw = G.solve(b, xa.copy(), method=method, precision=precision, tol=1e-10, x0_given=1)
+    assert rw["converged"] and _relres(A, xw, b) <= 1.0001e-10
+    assert rw["iterations"] < rc["iterations"], (rw["iterations"], rc["iterations"])
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.from_numpy(xa).cuda()
+    xd, rd = G.solve(bd, xd, method=method, precision=precision, tol=1e-10, x0_given=1)
+    assert rd["iterations"] == rw["iterations"]
+    np.testing.assert_array_equal(xd.cpu().numpy(), xw)
