@@ -1972,7 +1972,9 @@ __device__ __forceinline__ SolverParams item_params(const BatchItem &it, const B
     return P;
 }
 
-template <int MODE, class Sync>
+// MAXNR: the widest interleave the launch was built for (8 with one block per
+// SM; 4 with two, whose items never exceed 4 columns).
+template <int MODE, int MAXNR, class Sync>
 __device__ __forceinline__ void item_solve(const SolverParams &P, const MultiParams &M, int nr, const Ctx &c,
                                            SharedM &sh, Sync &sy)
 {
@@ -1980,12 +1982,17 @@ __device__ __forceinline__ void item_solve(const SolverParams &P, const MultiPar
     case 1: cg_multi_body<MODE, 1>(P, M, c, sh, sy); break;
     case 2: cg_multi_body<MODE, 2>(P, M, c, sh, sy); break;
     case 4: cg_multi_body<MODE, 4>(P, M, c, sh, sy); break;
-    default: cg_multi_body<MODE, 8>(P, M, c, sh, sy); break;
+    default:
+        if constexpr (MAXNR >= 8) cg_multi_body<MODE, 8>(P, M, c, sh, sy);
+        break;
     }
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
+// LB: resident blocks per SM the launch is built for (1: up to 128 registers a
+// thread, the widest items without spills; 2: 64 registers, twice the warps to
+// hide latency, for items of up to 4 columns).  The tuner picks.
+template <int MODE, int LB>
+__global__ void __launch_bounds__(kThreads, LB) k_batch(BatchParams B)
 {
     __shared__ SharedM sh;
     __shared__ TeamShared ts;
@@ -2011,7 +2018,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
         __syncthreads();
         const unsigned long long t0 = mf_globaltimer();
         TeamSync sy{sh, ts};
-        item_solve<MODE>(P, M, it.nr, c, sh, sy);
+        item_solve<MODE, (LB == 1 ? 8 : 4)>(P, M, it.nr, c, sh, sy);
         __syncthreads();
         if (ent.y == 0 && threadIdx.x == 0) {         // the item's start and end, for the report
             M.out[4 * it.nr + 3] = (double)t0;
@@ -2031,7 +2038,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_batch(BatchParams B)
         BlockSync sy{sh};
         const MultiParams M = it.M;
         const unsigned long long t0 = mf_globaltimer();
-        item_solve<MODE>(P, M, it.nr, c, sh, sy);
+        item_solve<MODE, (LB == 1 ? 8 : 4)>(P, M, it.nr, c, sh, sy);
         __syncthreads();
         if (threadIdx.x == 0) {
             M.out[4 * it.nr + 3] = (double)t0;
@@ -2672,7 +2679,8 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
 namespace {
 
 struct BatchImpl {
-    int dev = 0, cap = 8, nitems = 0, nsm = 0, max_res = 0;
+    int dev = 0, cap = 8, lb = 1, nitems = 0, nsm = 0;
+    int max_res[3] = {0, 0, 0};        // co-resident blocks of the k_batch<*, lb> launch, lb = 1, 2
     std::vector<mf_matrix_s *> sys;
     std::vector<int> nrhs;
     // items: system, first column, columns, interleave width, team size
@@ -2772,10 +2780,11 @@ void batch_schedule(const std::vector<double> &cost, const std::vector<int> &til
 // Items for column cap `cap`: each system's right-hand sides in groups of <= cap,
 // interleave width the next power of two (1, 2, 4, 8); team sizes and the
 // schedule; all vectors in one pool.
-int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
+int batch_build_items(BatchImpl &B, int cap, int lb, cudaStream_t s)
 {
     B.release_items();
     B.cap = cap;
+    B.lb = lb;
     B.it_sys.clear(); B.it_col0.clear(); B.it_ncol.clear(); B.it_nr.clear();
     for (int k = 0; k < (int)B.sys.size(); k++)
         for (int c0 = 0; c0 < B.nrhs[k]; c0 += cap) {
@@ -2803,8 +2812,8 @@ int batch_build_items(BatchImpl &B, int cap, cudaStream_t s)
         cost[t] = mf_batch_item_cost(A->nnz, A->n_rows, B.it_nr[t]);
         tilem[t] = A->tilem;
     }
-    // one block per SM (all resident: the launch is cooperative)
-    B.grid = std::max(1, std::min(B.max_res, B.nsm));
+    // lb blocks per SM (all resident: the launch is cooperative)
+    B.grid = std::max(1, std::min(B.max_res[lb], lb * B.nsm));
     std::vector<int> bptr, queue;
     std::vector<int2> blist;
     batch_schedule(cost, tilem, B.grid, B.it_team, bptr, blist, queue);
@@ -2908,8 +2917,13 @@ int batch_enqueue(BatchImpl &B, const double *const *Bd, double *const *Xd, cons
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (mode == MODE_FP64) MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_FP64>, bp));
-    else MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_MIXED>, bp));
+    if (B.lb == 2) {
+        if (mode == MODE_FP64) MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_FP64, 2>, bp));
+        else MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_MIXED, 2>, bp));
+    } else {
+        if (mode == MODE_FP64) MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_FP64, 1>, bp));
+        else MF_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_batch<MODE_MIXED, 1>, bp));
+    }
     for (int t = 0; t < B.nitems; t++) {
         const mf_matrix_s *A = B.sys[B.it_sys[t]];
         const int nr = B.it_nr[t], g = B.it_col0[t] / nr;
@@ -2935,13 +2949,16 @@ int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems
         cudaDeviceGetAttribute(&B.nsm, cudaDevAttrMultiProcessorCount, B.dev) != cudaSuccess)
         rc = MF_ERR_CUDA;
     if (rc == MF_SUCCESS) {
-        // co-resident blocks of the cooperative launch (both precisions)
-        int o64 = 0, o32 = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o64, k_batch<MODE_FP64>, kThreads, 0) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o32, k_batch<MODE_MIXED>, kThreads, 0) != cudaSuccess ||
-            std::min(o64, o32) < 1)
+        // co-resident blocks of the cooperative launch (both precisions, both register budgets)
+        int o[4] = {0, 0, 0, 0};
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[0], k_batch<MODE_FP64, 1>, kThreads, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[1], k_batch<MODE_MIXED, 1>, kThreads, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[2], k_batch<MODE_FP64, 2>, kThreads, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[3], k_batch<MODE_MIXED, 2>, kThreads, 0) != cudaSuccess ||
+            std::min(o[0], o[1]) < 1)
             rc = MF_ERR_CUDA;
-        B.max_res = std::min(o64, o32) * B.nsm;
+        B.max_res[1] = std::min(o[0], o[1]) * B.nsm;
+        B.max_res[2] = std::min(o[2], o[3]) * B.nsm;   // 0 if two blocks do not fit: never chosen
     }
     for (int k = 0; rc == MF_SUCCESS && k < nsys; k++) {
         if (!systems[k] || nrhs[k] < 1 || systems[k]->n_rows != systems[k]->n_cols || systems[k]->dev != B.dev) {
@@ -2956,7 +2973,7 @@ int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems
          cudaEventCreateWithFlags(&B.e_in, cudaEventDisableTiming) != cudaSuccess ||
          cudaStreamCreateWithFlags(&B.own, cudaStreamNonBlocking) != cudaSuccess))
         rc = MF_ERR_CUDA;
-    if (rc == MF_SUCCESS) rc = batch_build_items(B, 8, s ? s : B.own);
+    if (rc == MF_SUCCESS) rc = batch_build_items(B, 8, 1, s ? s : B.own);
     if (rc != MF_SUCCESS) {
         mf_batch_destroy_impl(b);
         return rc;
@@ -3023,6 +3040,7 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
         }
         const double opts[] = {opt->tol, (double)opt->max_iter, (double)opt->fixed_iters, (double)opt->replace_every,
                                opt->demote_fp16, opt->demote_int8, (double)opt->use_lossless, (double)B.cap,
+                               (double)B.lb,
                                opt->wait_timeout_s, (double)opt->test_stall_barrier, opt->demote_min_fraction};
         for (double v : opts) {
             unsigned long long u;
@@ -3123,11 +3141,15 @@ int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cud
     o.fixed_iters = 1;
     o.max_iter = iters;
     o.replace_every = 0;
-    int best = 8;
+    // (columns per item, blocks per SM): two blocks per SM only for items of up
+    // to 4 columns (8-column items need the 128-register budget)
+    const int cand[][2] = {{8, 1}, {4, 1}, {2, 1}, {4, 2}, {2, 2}};
+    int best = 8, best_lb = 1;
     double best_ms = 1e300;
-    for (int cap : {8, 4, 2}) {
+    for (const auto &cl : cand) {
         if (rc != MF_SUCCESS) break;
-        if ((rc = batch_build_items(B, cap, run)) != MF_SUCCESS) break;
+        if (cl[1] == 2 && B.max_res[2] < 1) continue;
+        if ((rc = batch_build_items(B, cl[0], cl[1], run)) != MF_SUCCESS) break;
         double ms = 0.0;
         for (int rep = 0; rep < 2 && rc == MF_SUCCESS; rep++) {   // the first run warms up
             rc = mf_batch_solve_impl(b, bufB.data(), bufX.data(), &o, nullptr, 0, run);
@@ -3135,12 +3157,13 @@ int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cud
         }
         if (rc == MF_SUCCESS && ms < best_ms) {
             best_ms = ms;
-            best = cap;
+            best = cl[0];
+            best_lb = cl[1];
         }
     }
     for (size_t k = 0; k < B.sys.size(); k++)
         if (bufB[k]) cudaFree(bufB[k]);
-    if (rc == MF_SUCCESS) rc = batch_build_items(B, best, run);
+    if (rc == MF_SUCCESS) rc = batch_build_items(B, best, best_lb, run);
     if (chosen) *chosen = best;
     return rc;
 }

@@ -44,6 +44,9 @@ def test_status_strings_and_defaults(mf):
     assert o.precision == mf.MF_PREC_MIXED and o.replace_every == 50 and o.tol == 1e-8
     o2 = mf.default_options(precision="fp64", method="bicgstab", tol=1e-10)
     assert o2.precision == 0 and o2.method == 1 and o2.tol == 1e-10
+    # the ctypes mirror of mf_options has the C layout: the last field is set by mf_options_default
+    assert o.demote_min_fraction == 0.125 and o.x0_given == 0 and o.l2_window == 1 and o.use_lossless == 1
+    assert o.demote_fp16 == 2.0 ** -13 and o.demote_int8 == 2.0 ** -16 and o.wait_timeout_s == 10.0
 
 
 def test_no_device_reports_not_built(mf):
