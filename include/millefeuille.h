@@ -218,16 +218,20 @@ int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_o
 /*
  * Batched solves: many independent square systems (each an mf_matrix on the
  * current device) with nrhs[k] right-hand sides each, in ONE persistent launch.
- * A device work queue holds (system, up to `cap` right-hand sides) items,
- * largest estimated cost first; each 512-thread block takes the next item and
- * solves it alone (CG, FP64 or mixed; block-level syncs), then the next.  No
- * counterpart in the reference (one system per call).
+ * Work items are (system, up to `cap` right-hand sides).  Items far above a
+ * fair share of the launch are solved by teams of 512-thread blocks on a host
+ * list schedule; the rest sit in a device work queue, largest estimated cost
+ * first, and a block takes the next one and solves it alone (CG, FP64 or
+ * mixed; block-level syncs).  One cooperative launch of one or two blocks per
+ * SM.  No counterpart in the reference (one system per call).
  *
  * mf_batch_create  keeps the handles' pointers (the matrices must outlive the
- *                  batch) and sizes the work items (cap 8).
- * mf_batch_tune    picks the right-hand sides per item (8, 4 or 2) by timing
- *                  `iters` fixed iterations of the real batch; *chosen_cap
- *                  (nullable) gets the choice.
+ *                  batch) and sizes the work items (cap 8, one block per SM).
+ * mf_batch_tune    picks the right-hand sides per item and the blocks per SM
+ *                  ((8,1), (4,1), (2,1), (4,2), (2,2)) by timing `iters` fixed
+ *                  iterations of the real batch; *chosen_cap (nullable) gets
+ *                  the right-hand sides per item (grid_blocks in the reports
+ *                  shows the blocks).
  * mf_batch_solve   B[k] / X[k]: DEVICE arrays of nrhs[k] x n_k doubles (one
  *                  vector after another).  reports (nullable): sum(nrhs)
  *                  records, system by system; time_ms is the whole batch's;

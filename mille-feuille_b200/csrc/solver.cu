@@ -1747,8 +1747,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_solve_multi(SolverParams P, Mul
 }
 
 // ------------------------------------------------------------ batched systems
-// Many independent systems in one persistent launch of one 512-thread block
-// per SM.  Work items are (system, up to 8 of its right-hand sides).
+// Many independent systems in one persistent launch of one or two 512-thread
+// blocks per SM (k_batch<MODE, LB>).  Work items are (system, up to 8 of its
+// right-hand sides).
 //  * Team items: an item whose estimated cost exceeds a fair share of the
 //    launch (total cost / blocks) is solved by a team of k blocks, sized by its
 //    cost; the host list-schedules team items onto blocks (the k blocks that
