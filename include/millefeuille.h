@@ -251,6 +251,18 @@ int mf_batch_solve(mf_batch b, const double *const *B, double *const *X, const m
 int mf_batch_destroy(mf_batch b);
 
 /*
+ * The team sizes and list schedule a batch launch of `grid` blocks uses for
+ * items of estimated cost cost[t] and tilem[t] tile-rows (host only; for
+ * inspection and tests).  team[t] (nitems): blocks solving item t (1: queue
+ * item).  bptr (grid + 1) and blist (2 ints per entry: item, rank in its team;
+ * at most sum(team) entries): block b's ordered team entries are
+ * blist[2*bptr[b] .. 2*bptr[b+1]).  queue (nitems): the queue items, largest
+ * cost first; *nqueue their count.  No counterpart in the reference.
+ */
+int mf_batch_schedule(int nitems, const double *cost, const int *tilem, int grid, int *team, int *bptr,
+                      int *blist, int *queue, int *nqueue);
+
+/*
  * Split of a batch's systems over nparts GPUs (one process per GPU, each with
  * its own mf_batch of the systems it owns; no collective on the data path).
  * Greedy longest-processing-time over whole systems, by decreasing estimated

@@ -367,6 +367,17 @@ extern "C" int mf_batch_destroy(mf_batch b)
     return MF_SUCCESS;
 }
 
+extern "C" int mf_batch_schedule(int nitems, const double *cost, const int *tilem, int grid, int *team, int *bptr,
+                                 int *blist, int *queue, int *nqueue)
+{
+    if (nitems < 0 || grid < 1 || (nitems > 0 && (!cost || !tilem || !team || !queue)) || !bptr || !nqueue ||
+        (nitems > 0 && !blist))
+        return MF_ERR_INVALID;
+    for (int t = 0; t < nitems; t++)
+        if (!(cost[t] >= 0.0) || tilem[t] < 0) return MF_ERR_INVALID;
+    return mf_batch_schedule_impl(nitems, cost, tilem, grid, team, bptr, blist, queue, nqueue);
+}
+
 // Greedy longest-processing-time split of whole systems over nparts GPUs: the
 // systems by decreasing cost (ties: lower index first), each to the part with
 // the least load so far (ties: lower part).  A system's cost is the sum over its

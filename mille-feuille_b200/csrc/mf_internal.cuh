@@ -139,6 +139,8 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
                         mf_report *reps, int use_graph, cudaStream_t s);
 int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cudaStream_t s);
 void mf_batch_destroy_impl(mf_batch_s *b);
+int mf_batch_schedule_impl(int nitems, const double *cost, const int *tilem, int grid, int *team, int *bptr,
+                           int *blist, int *queue, int *nqueue);
 int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s,
                 double *elapsed_ms);
 int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s);

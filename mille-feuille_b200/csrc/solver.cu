@@ -2937,6 +2937,25 @@ int batch_enqueue(BatchImpl &B, const double *const *Bd, double *const *Xd, cons
 
 }  // namespace
 
+// The batch's team sizes and list schedule for given item costs (host only).
+int mf_batch_schedule_impl(int nitems, const double *cost, const int *tilem, int grid, int *team, int *bptr,
+                           int *blist, int *queue, int *nqueue)
+{
+    std::vector<double> c(cost, cost + nitems);
+    std::vector<int> tm(tilem, tilem + nitems), tv, bp, q;
+    std::vector<int2> bl;
+    batch_schedule(c, tm, grid, tv, bp, bl, q);
+    for (int t = 0; t < nitems; t++) team[t] = tv[t];
+    for (int b = 0; b <= grid; b++) bptr[b] = bp[b];
+    for (size_t e = 0; e < bl.size(); e++) {
+        blist[2 * e] = bl[e].x;
+        blist[2 * e + 1] = bl[e].y;
+    }
+    for (size_t k = 0; k < q.size(); k++) queue[k] = q[k];
+    *nqueue = (int)q.size();
+    return MF_SUCCESS;
+}
+
 struct mf_batch_s {
     BatchImpl impl;
 };

@@ -306,6 +306,27 @@ class Batch:
             pass
 
 
+def batch_schedule(cost, tilem, grid: int):
+    """The team sizes and list schedule a batch launch of `grid` blocks uses
+    (mf_batch_schedule): (team per item, per-block lists of (item, rank),
+    queue items largest first)."""
+    L = _lib.load()
+    n = len(cost)
+    c = np.ascontiguousarray(cost, dtype=np.float64)
+    t = np.ascontiguousarray(tilem, dtype=np.int32)
+    team = np.zeros(max(n, 1), np.int32)
+    bptr = np.zeros(grid + 1, np.int32)
+    blist = np.zeros(2 * max(1, n * grid), np.int32)
+    queue = np.zeros(max(n, 1), np.int32)
+    nq = C.c_int()
+    I = C.POINTER(C.c_int)
+    check(L.mf_batch_schedule(n, c.ctypes.data_as(C.POINTER(C.c_double)), t.ctypes.data_as(I), int(grid),
+                              team.ctypes.data_as(I), bptr.ctypes.data_as(I), blist.ctypes.data_as(I),
+                              queue.ctypes.data_as(I), C.byref(nq)), "mf_batch_schedule")
+    lists = [[(int(blist[2 * e]), int(blist[2 * e + 1])) for e in range(bptr[b], bptr[b + 1])] for b in range(grid)]
+    return [int(v) for v in team[:n]], lists, [int(v) for v in queue[:nq.value]]
+
+
 def read_matrix(path: str):
     """Reads .mtx / .cbd with the reference's semantics; returns
     (m, n, rowptr, colidx, val, is_symmetric) as numpy arrays."""

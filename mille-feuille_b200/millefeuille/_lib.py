@@ -66,7 +66,7 @@ EXPORTED = [
     "mf_matrix_destroy", "mf_matrix_get_info", "mf_tile_array_bytes", "mf_tile_export", "mf_solve", "mf_spmv",
     "mf_debug_ref_labels", "mf_build_arch", "mf_spmv_noalloc", "mf_value_grad", "mf_matrix_create_transposed",
     "mf_solve_multi", "mf_batch_create", "mf_batch_tune", "mf_batch_solve", "mf_batch_destroy",
-    "mf_batch_partition",
+    "mf_batch_partition", "mf_batch_schedule",
 ]
 
 _lib = None
@@ -100,6 +100,7 @@ def load() -> C.CDLL:
                                  vp]
     L.mf_batch_destroy.argtypes = [vp]
     L.mf_batch_partition.argtypes = [C.c_int, ip, C.POINTER(C.c_longlong), ip, C.c_int, C.c_int, ip, dp]
+    L.mf_batch_schedule.argtypes = [C.c_int, dp, ip, C.c_int, ip, ip, ip, ip, ip]
     L.mf_matrix_create_transposed.argtypes = [C.POINTER(vp), vp, vp]
     L.mf_debug_ref_labels.argtypes = [vp, vp, C.c_int, vp, C.c_int]
     L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
