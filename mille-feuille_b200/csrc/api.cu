@@ -326,6 +326,7 @@ extern "C" int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X,
         MF_CUDA_TRY(cudaMemcpyAsync(tmp, B, bytes, cudaMemcpyHostToDevice, s));
         dB = tmp;
         dX = tmp + (size_t)nrhs * A->n_rows;
+        if (o.x0_given) MF_CUDA_TRY(cudaMemcpyAsync(dX, X, bytes, cudaMemcpyHostToDevice, s));
     }
     int rc = mf_solver_multi_run(A, nrhs, dB, dX, &o, reports, s);
     if (!device_ptrs) {

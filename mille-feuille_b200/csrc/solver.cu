@@ -185,9 +185,10 @@ __device__ __forceinline__ int parity_prec(int code)
     return code == 0 ? MF_P64 : code == 4 ? MF_P32 : code == 3 ? MF_P16 : code == 2 ? MF_P8 : MF_PSKIP;
 }
 
-// The x operands of one SpMV: FP64 vector, its FP32 shadow, and (parity mode)
-// its FP16 / INT8 shadows; mag / lab are the per-column-segment statistics the
-// precision choice reads.
+// The x operands of one SpMV: the FP64 vector (FP64 and mixed modes multiply
+// every stored precision against it), and in parity mode its FP32 / FP16 /
+// INT8 shadows; mag / lab are the per-column-segment statistics the precision
+// choice reads.
 struct XVec {
     const double *x64;
     const float *x32;
@@ -1477,27 +1478,71 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
     for (int R = c.rbeg; R < c.rend && !has_empty; R++) has_empty = P.seg_ptr[R] == P.seg_ptr[R + 1];
     const unsigned mm2 = 3u << NR;          // the two trailing max slots
 
-    // ---- init: X = 0, R = B, P = Q = 0; |b_k|^2; R's shadow ----
-    double pb[NR + 2];
+    // ---- init: X = 0, R = B, P = Q = 0; |b_k|^2; R's segment magnitudes ----
+    // With an initial guess (x0_given): |b_k|^2 reduced first (it scales the
+    // convergence test), then R = B - A X in FP64.
+    double pb[NR + 2], bb0[NR];
 #pragma unroll
     for (int k = 0; k < NR + 2; k++) pb[k] = 0.0;
     SegMM st = {0.0f, 3.0e38f};
-    for (int R = c.rbeg; R < c.rend; R++) {
-        const int row = R * MF_BS + c.i;
-        const bool valid = row < n;
-        double rv[NR], z[NR];
+    if (P.x0_given) {
+        double pbb[NR];
 #pragma unroll
-        for (int k = 0; k < NR; k++) { rv[k] = 0.0; z[k] = 0.0; }
-        if (valid) {
-            load_row<NR>(M.B, row, rv);
-            store_row<NR>(M.X, row, z);
-            store_row<NR>(M.R, row, rv);
-            store_row<NR>(M.Pv, row, z);
-            store_row<NR>(M.Q, row, z);
+        for (int k = 0; k < NR; k++) pbb[k] = 0.0;
+        for (int R = c.rbeg; R < c.rend; R++) {
+            const int row = R * MF_BS + c.i;
+            if (row < n) {
+                double bv[NR];
+                load_row<NR>(M.B, row, bv);
 #pragma unroll
-            for (int k = 0; k < NR; k++) pb[k] += rv[k] * rv[k];
+                for (int k = 0; k < NR; k++) pbb[k] += bv[k] * bv[k];
+            }
         }
-        publish_multi<MODE, NR>(M, R, row, valid, rv, st, c.hmask);
+        if (!sy.template reduce<NR>(8, pbb, 0u, bb0)) return;
+        auto init_r = [&](int R, const double (&y)[NR]) {
+            const int row = R * MF_BS + c.i;
+            const bool valid = row < n;
+            double rv[NR], z[NR];
+#pragma unroll
+            for (int k = 0; k < NR; k++) { rv[k] = 0.0; z[k] = 0.0; }
+            if (valid) {
+                load_row<NR>(M.B, row, rv);
+#pragma unroll
+                for (int k = 0; k < NR; k++) rv[k] -= y[k];
+                store_row<NR>(M.R, row, rv);
+                store_row<NR>(M.Pv, row, z);
+                store_row<NR>(M.Q, row, z);
+#pragma unroll
+                for (int k = 0; k < NR; k++) pb[k] += rv[k] * rv[k];
+            }
+            publish_multi<MODE, NR>(M, R, row, valid, rv, st, c.hmask);
+        };
+        spmv_multi<MODE, NR, true>(P, c.sbeg, c.send, c.i, c.hmask, M.X, nullptr, 0.0f, 1, init_r);
+        if (has_empty) {
+            double zy[NR];
+#pragma unroll
+            for (int k = 0; k < NR; k++) zy[k] = 0.0;
+            for (int R = c.rbeg; R < c.rend; R++)
+                if (P.seg_ptr[R] == P.seg_ptr[R + 1]) init_r(R, zy);
+        }
+    } else {
+        for (int R = c.rbeg; R < c.rend; R++) {
+            const int row = R * MF_BS + c.i;
+            const bool valid = row < n;
+            double rv[NR], z[NR];
+#pragma unroll
+            for (int k = 0; k < NR; k++) { rv[k] = 0.0; z[k] = 0.0; }
+            if (valid) {
+                load_row<NR>(M.B, row, rv);
+                store_row<NR>(M.X, row, z);
+                store_row<NR>(M.R, row, rv);
+                store_row<NR>(M.Pv, row, z);
+                store_row<NR>(M.Q, row, z);
+#pragma unroll
+                for (int k = 0; k < NR; k++) pb[k] += rv[k] * rv[k];
+            }
+            publish_multi<MODE, NR>(M, R, row, valid, rv, st, c.hmask);
+        }
     }
     pb[NR] = st.mx;
     pb[NR + 1] = -st.mn;
@@ -1505,9 +1550,9 @@ __device__ void cg_multi_body(const SolverParams &P, const MultiParams &M, const
     if (!sy.template reduce<NR + 2>(0, pb, mm2, v)) return;
     if (threadIdx.x == 0) {
         for (int k = 0; k < NR; k++) {
-            sh.bb[k] = v[k];
+            sh.bb[k] = P.x0_given ? bb0[k] : v[k];
             sh.rr[k] = v[k];
-            sh.thr2[k] = P.tol * P.tol * v[k];
+            sh.thr2[k] = P.tol * P.tol * sh.bb[k];
             sh.beta[k] = 0.0;
             sh.pending[k] = 0;
             sh.iters[k] = 0;
@@ -1962,6 +2007,7 @@ __device__ __forceinline__ SolverParams item_params(const BatchItem &it, const B
     P.v8 = it.v8;
     P.i8_scale = it.i8_scale;
     P.max_iter = B.max_iter;
+    P.x0_given = 0;
     P.fixed_iters = B.fixed_iters;
     P.replace_every = B.replace_every;
     P.use_lossless = B.use_lossless;
@@ -2600,7 +2646,6 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
                         mf_report *reps, cudaStream_t s)
 {
     if (opt->method != MF_METHOD_CG || opt->precision == MF_PREC_PARITY) return MF_ERR_UNSUPPORTED;
-    if (opt->x0_given) return MF_ERR_UNSUPPORTED;
     const int mode = opt->precision == MF_PREC_FP64 ? MODE_FP64 : MODE_MIXED;
     Workspace *w = nullptr;
     MF_TRY(ws_get(A, opt->blocks_per_sm, &w, s));
@@ -2612,6 +2657,7 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
     fill_params(P, A, w);
     P.hw_begin = w->m_hw_begin;
     P.method = MF_METHOD_CG;
+    P.x0_given = opt->x0_given ? 1 : 0;
     P.max_iter = opt->max_iter;
     P.fixed_iters = opt->fixed_iters;
     P.replace_every = opt->replace_every;
@@ -2638,6 +2684,7 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
     for (int g = 0; g < groups; g++) {
         M.nr = std::min(nr, nrhs - g * nr);
         k_interleave<<<592, 256, 0, s>>>(d_B, n, (int)L, nrhs, g, nr, (double *)M.B);
+        if (opt->x0_given) k_interleave<<<592, 256, 0, s>>>(d_X, n, (int)L, nrhs, g, nr, M.X);
         MF_CUDA_TRY(cudaGetLastError());
         MF_CUDA_TRY(cudaMemsetAsync(w->bar, 0, sizeof(unsigned int), s));
         MF_CUDA_TRY(cudaMemsetAsync(w->err, 0, sizeof(int), s));
