@@ -125,6 +125,34 @@ def algorithmic_bytes(rep, n, nnz, tilenum, method="cg"):
     return mat + vec + repl
 
 
+def verify(A, x, b, x_ref=None):
+    """Independent FP64 check of a returned solution on the host (scipy):
+    relative residual ||b - A x|| / ||b|| and, when a reference solution is
+    known, the forward error ||x - x_ref|| / ||x_ref||."""
+    import numpy as np
+    out = {"relres_host_check": float(np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b))}
+    if x_ref is not None:
+        out["fwd_err"] = float(np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref))
+    return out
+
+
+def precisions_used(rep):
+    names = ("f64", "f32", "f16", "i8")
+    return [nm for nm, c in zip(names, rep["tile_uses"]) if c > 0] or ["f64"]
+
+
+def spmv_timed(G, xs, ys, precision, warmup, reps, flush, sp):
+    """Median CUDA-event time of the standalone tile SpMV, L2 flushed (a
+    256 MB write, larger than the 126 MB L2) before every launch."""
+    ts = []
+    for i in range(warmup + reps):
+        flush.fill_(float(i))
+        G.spmv(xs, ys, precision=precision, stream=sp)
+        if i >= warmup:
+            ts.append(G.last_spmv_ms)
+    return statistics.median(ts)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -172,33 +200,34 @@ def run_ours(args, rank, world, local_rank):
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        return ms, reps
+        return ms, reps, (hx if host else None)
 
     for _ in range(args.warmup):
         G.solve(bd, xd, options=mixed, stream=sp)
     with ClockSampler(local_rank) as clk:
-        ms_mixed, reps = timed(mixed, args.steps)
+        ms_mixed, reps, _ = timed(mixed, args.steps)
     rep = reps[-1]
+    # the mixed solution is read back before anything else writes xd
+    chk_mixed = verify(A, xd.cpu().numpy(), b, x_true)
     # the same kernel in all-FP64
     G.solve(bd, xd, options=fp64, stream=sp)
-    ms_fp64, reps64 = timed(fp64, max(1, args.steps))
+    ms_fp64, reps64, _ = timed(fp64, max(1, args.steps))
     rep64 = reps64[-1]
+    chk_fp64 = verify(A, xd.cpu().numpy(), b, x_true)
     # end to end through the public API with host buffers (H2D b, D2H x each step)
     G.solve(b, np.zeros_like(b), options=mixed, stream=sp)
-    ms_e2e, _ = timed(mixed, args.steps, host=True)
-    # standalone FP64 tile SpMV, L2 flushed between launches
+    ms_e2e, reps_e2e, hx = timed(mixed, args.steps, host=True)
+    chk_e2e = verify(A, np.array(hx), b, x_true)
+    # standalone tile SpMV in FP64 and with every tile in FP32, L2 flushed between launches
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     xs = torch.from_numpy(np.random.default_rng(7).uniform(-1, 1, A.n)).to(dev)
     ys = torch.empty_like(xs)
-    spmv_ms = []
-    for i in range(args.warmup + 10):
-        flush.fill_(float(i))
-        G.spmv(xs, ys, precision="fp64", stream=sp)
-        if i >= args.warmup:
-            spmv_ms.append(G.last_spmv_ms)
-    spmv_t = statistics.median(spmv_ms)
+    spmv64 = spmv_timed(G, xs, ys, "fp64", args.warmup, 10, flush, sp)
+    spmv32 = spmv_timed(G, xs, ys, "mixed", args.warmup, 10, flush, sp)
+    del flush
     n, nnz, T = A.n, A.nnz, info["tilenum"]
-    b_spmv = 9 * nnz + 8 * T + 16 * n
+    b_spmv64 = 9 * nnz + 8 * T + 16 * n
+    b_spmv32 = 5 * nnz + 8 * T + 16 * n
     peak, peak_kind = _peaks()
     alg = algorithmic_bytes(rep, n, nnz, T)
     achieved = alg / (rep["time_ms"] * 1e-3) / 1e9
@@ -213,38 +242,50 @@ def run_ours(args, rank, world, local_rank):
             traffic = int(tj["dram_bytes_per_launch"] * rep["iterations"] / tj["iterations"])
         except Exception:
             traffic = None
-    # independent FP64 check of the returned solution (host, scipy)
-    x = xd.cpu().numpy()
-    relres_host = float(np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b))
     value = ms_mixed / world
+    gbs = lambda nbytes, ms: round(nbytes / (ms * 1e-3) / 1e9, 1)
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_mixed, 4), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 dots/updates, f32/f16/i8 tile products",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 vectors, dots, updates and products; matrix values stored "
+                 + "/".join(precisions_used(rep)) + " and widened to f64",
         "data": "synthetic (seeded generator, no dataset)",
         "config": {
             "workload": WORKLOAD, "n": n, "nnz": nnz, "tiles": T, "tol": TOL, "replace_every": 50,
             "parallelism": f"replicas x{world} (one system per GPU)",
             "l2": f"inputs larger than L2: slice payload {round(info['slice_entries'] * 16 / 1e6)} MB per solve",
             "iterations_mixed": rep["iterations"], "relres_true_mixed": rep["relres_true"],
-            "relres_host_check": relres_host, "fp64_ms": round(ms_fp64, 4),
+            "relres_host_check_mixed": chk_mixed["relres_host_check"], "fwd_err_mixed": chk_mixed["fwd_err"],
+            "fp64_ms": round(ms_fp64, 4),
             "iterations_fp64": rep64["iterations"], "relres_true_fp64": rep64["relres_true"],
+            "relres_host_check_fp64": chk_fp64["relres_host_check"], "fwd_err_fp64": chk_fp64["fwd_err"],
             "mixed_vs_fp64_speedup": round(ms_fp64 / ms_mixed, 3),
             "kernel_ms_mixed": rep["time_ms"], "kernel_ms_fp64": rep64["time_ms"],
-            "tile_uses": rep["tile_uses"], "nnz_uses": rep["nnz_uses"],
-            "spmv_fp64_ms": round(spmv_t, 5), "spmv_fp64_gbs": round(b_spmv / (spmv_t * 1e-3) / 1e9, 1),
-            "spmv_frac_of_hbm": round(b_spmv / (spmv_t * 1e-3) / 1e9 / peak, 3),
+            "us_per_iteration_mixed": round(rep["time_ms"] * 1e3 / max(1, rep["iterations"]), 2),
+            "us_per_iteration_fp64": round(rep64["time_ms"] * 1e3 / max(1, rep64["iterations"]), 2),
+            "tile_uses": rep["tile_uses"], "nnz_uses": rep["nnz_uses"], "replacements": rep["replacements"],
+            "spmv_fp64_ms": round(spmv64, 5), "spmv_fp64_gbs": gbs(b_spmv64, spmv64),
+            "spmv_frac_of_hbm": round(b_spmv64 / (spmv64 * 1e-3) / 1e9 / peak, 3),
+            "spmv_fp32_ms": round(spmv32, 5), "spmv_fp32_gbs": gbs(b_spmv32, spmv32),
+            "spmv_fp32_frac_of_hbm": round(b_spmv32 / (spmv32 * 1e-3) / 1e9 / peak, 3),
             "grid": [rep["grid_blocks"], rep["threads_per_block"]], "build_ms": info["build_ms"],
+            "phase_ms_mixed": rep["phase_ms"],
         },
         "e2e": {"value": round(ms_e2e / world, 4), "unit": "ms", "h2d_bytes_per_step": 8 * n,
-                "d2h_bytes_per_step": 8 * n},
+                "d2h_bytes_per_step": 8 * n, "relres_host_check": chk_e2e["relres_host_check"],
+                "fwd_err": chk_e2e["fwd_err"], "host_ms": reps_e2e[-1].get("host_ms")},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 3), "traffic": traffic,
+                     "dram_gbs": round(traffic / (rep["time_ms"] * 1e-3) / 1e9, 1) if traffic else None,
+                     "dram_frac": round(traffic / (rep["time_ms"] * 1e-3) / 1e9 / peak, 3) if traffic else None,
                      "kernel": "k_solve<MIXED> (persistent CG)", "peak_kind": f"{peak_kind} hbm_gbs",
                      "algorithmic_bytes_per_launch": alg},
         "clocks": clk.summary(),
     }
+    if not args.no_c1:
+        out["config"]["laplace2d_256"] = c1_line(dev, args.steps)
     if not args.no_bicgstab:
         out["config"]["bicgstab"] = bicgstab_line(dev, args.steps)
     if not args.no_adjoint:
@@ -255,6 +296,36 @@ def run_ours(args, rank, world, local_rank):
         out["cpu_baseline"] = cpu_baseline(A, b, rep64["iterations"], budget_s=args.cpu_budget)
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def c1_line(dev, steps):
+    """The 2D 5-point Laplacian on 256^2 (n = 65,536; b = A x_true, x_true ~
+    U(-1,1) seed 0, x0 = 0): CG to 1e-10 in FP64 (max 10,000 iterations, the
+    plain-CG configuration) and in mixed precision.  About 4 MB of matrix per
+    SpMV sits in L2, so the solve is bound by the grid syncs: reported in us
+    per iteration.  One untimed solve each, then the best of `steps`."""
+    import torch
+    import millefeuille as mf
+    from millefeuille import matrices as M
+    A, b, xt = M.laplace2d_system(256, seed=0)
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    bd = torch.from_numpy(b).to(dev)
+    xd = torch.zeros_like(bd)
+    out = {"workload": f"laplace2d_256 (n={A.n}, nnz={A.nnz}), CG tol 1e-10, max 10000 iterations"}
+    for prec in ("fp64", "mixed"):
+        o = mf.default_options(precision=prec, tol=1e-10, max_iter=10000, replace_every=0 if prec == "fp64" else 50)
+        G.solve(bd, xd, options=o)
+        best = None
+        for _ in range(max(1, steps)):
+            _, r = G.solve(bd, xd, options=o)
+            if best is None or r["time_ms"] < best["time_ms"]:
+                best = r
+        d = {"ms": round(best["time_ms"], 3), "iterations": best["iterations"],
+             "us_per_iteration": round(best["time_ms"] * 1e3 / max(1, best["iterations"]), 2),
+             "relres_true": best["relres_true"]}
+        d.update(verify(A, xd.cpu().numpy(), b, xt))
+        out[prec] = d
+    return out
 
 
 def batch_line(dev, nsys, rank=0, world=1):
@@ -327,6 +398,11 @@ def bicgstab_line(dev, steps):
     bd = torch.from_numpy(b).to(dev)
     xd = torch.zeros_like(bd)
     out = {"workload": f"convdiff3d_96 (n={A.n}, nnz={A.nnz}, max cell Peclet {pe:.2f}), BiCGSTAB tol 1e-8"}
+    # reference solution for the forward error (b = A 1 + noise has no closed form):
+    # FP64 BiCGSTAB to 1e-12 on the same kernel
+    G.solve(bd, xd, options=mf.default_options(method="bicgstab", precision="fp64", tol=1e-12, replace_every=0))
+    x_ref = xd.cpu().numpy()
+    out["fwd_err_reference"] = "FP64 BiCGSTAB to relres 1e-12"
     for prec in ("mixed", "fp64"):
         o = mf.default_options(method="bicgstab", precision=prec, tol=TOL, replace_every=50 if prec == "mixed" else 0)
         G.solve(bd, xd, options=o)
@@ -335,10 +411,9 @@ def bicgstab_line(dev, steps):
             _, r = G.solve(bd, xd, options=o)
             if best is None or r["time_ms"] < best["time_ms"]:
                 best = r
-        x = xd.cpu().numpy()
         out[prec] = {"ms": round(best["time_ms"], 3), "iterations": best["iterations"],
-                     "relres_true": best["relres_true"],
-                     "relres_host_check": float(np.linalg.norm(A.to_scipy() @ x - b) / np.linalg.norm(b))}
+                     "relres_true": best["relres_true"], "tile_uses": best["tile_uses"]}
+        out[prec].update(verify(A, xd.cpu().numpy(), b, x_ref))
     out["mixed_vs_fp64_speedup"] = round(out["fp64"]["ms"] / out["mixed"]["ms"], 3)
     return out
 
@@ -387,23 +462,33 @@ def fwd_adjoint(dev, nrhs):
 
 
 def cpu_baseline(A, b, iters_to_tol, budget_s=12.0):
-    """The reference's CPU path restated (oracle FP64 tile-SpMV CG) on all host
-    threads: a bounded sample of iterations, scaled to the iteration count."""
+    """The reference's CPU path restated (oracle FP64 tile-SpMV CG) on the host
+    cores: a bounded sample of iterations on all host threads (the headline
+    column), and a second bounded sample on one core, the reference's serial
+    loop as written; each scaled to the FP64 iteration count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     threads = os.cpu_count() or 1
     T = oracle.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
-    T.cg_fp64(b, max_iter=5, fixed_iters=True, nthreads=threads)
-    done, t_total = 0, 0.0
-    while t_total < budget_s and done < 2000:
-        t0 = time.perf_counter()
-        T.cg_fp64(b, max_iter=50, fixed_iters=True, nthreads=threads)
-        t_total += time.perf_counter() - t0
-        done += 50
-    ms_it = t_total * 1e3 / done
+
+    def sample(nthreads, chunk, budget):
+        T.cg_fp64(b, max_iter=min(5, chunk), fixed_iters=True, nthreads=nthreads)
+        done, t_total = 0, 0.0
+        while t_total < budget and done < 2000:
+            t0 = time.perf_counter()
+            T.cg_fp64(b, max_iter=chunk, fixed_iters=True, nthreads=nthreads)
+            t_total += time.perf_counter() - t0
+            done += chunk
+        return t_total * 1e3 / done, done
+
+    ms_it, done = sample(threads, 50, budget_s)
+    ms_1, done_1 = sample(1, 5, budget_s / 2)
     return {"value": round(ms_it * iters_to_tol, 2), "unit": "ms", "cores": threads, "kind": "port",
             "sample": f"{done} FP64 tile-SpMV CG iterations of the 128^3 system (restated reference CPU path), "
-                      f"{ms_it:.2f} ms/iteration x {iters_to_tol} iterations to 1e-8"}
+                      f"{ms_it:.2f} ms/iteration x {iters_to_tol} iterations to 1e-8",
+            "serial_1core": {"value": round(ms_1 * iters_to_tol, 1), "unit": "ms", "cores": 1,
+                             "ms_per_iteration": round(ms_1, 2),
+                             "sample": f"{done_1} iterations on one core, scaled to {iters_to_tol}"}}
 
 
 def run_reference(args, rank, world):
@@ -493,6 +578,7 @@ def main():
     ap.add_argument("--adjoint-rhs", type=int, default=32)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-solves line")
     ap.add_argument("--no-bicgstab", action="store_true", help="skip the BiCGSTAB (convection-diffusion) line")
+    ap.add_argument("--no-c1", action="store_true", help="skip the 2D 256^2 Laplacian CG line")
     ap.add_argument("--batch-systems", type=int, default=512)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     args = ap.parse_args()

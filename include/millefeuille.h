@@ -156,6 +156,10 @@ typedef struct {
     double phase_ms[6];    /* block 0's wall time split: SpMV phases, first vector update,
                               direction update, barriers + reductions, FP64 residual replacement;
                               [5]: of the barrier time, block 0 spinning for the other blocks */
+    double host_ms[4];     /* mf_solve's host-side wall time: [0] staging buffer and H2D copy of b
+                              enqueued (host pointers), [1] solver state zeroed and L2 window set,
+                              [2] launch until the results are read back (includes the kernel),
+                              [3] D2H copy of x and the closing synchronisation (host pointers) */
 } mf_report;
 
 void mf_options_default(mf_options *opt);
@@ -170,6 +174,7 @@ typedef struct {
     int nseg;               /* solver slices */
     long long slice_entries;/* padded solver entries */
     double build_ms;        /* GPU tiling + encoding time */
+    int device;             /* CUDA device the handle's memory lives on (current at create) */
 } mf_matrix_info;
 
 /*
@@ -300,10 +305,15 @@ int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_p
  *    MF_ERR_UNSUPPORTED before anything is launched.
  *  - Nothing has to start at zero: each call writes every scratch entry the
  *    kernel reads (x, then zeros up to the padded length).
+ *  - The current device must be the one the matrix was created on
+ *    (mf_matrix_info.device); otherwise the call returns MF_ERR_INVALID.
  *  - The first call on a device looks the buffer up (cudaGetSymbolAddress,
  *    which may load the library's device code); make that first call before
  *    any stream capture.  Later calls only issue a copy, a memset and the
- *    kernel.
+ *    kernel.  The address is kept for the life of the loaded library: a
+ *    cudaDeviceReset in the caller's process unloads the device code and
+ *    leaves it stale, so after a reset the library must be unloaded and
+ *    loaded again before this entry point is called.
  *  - One buffer per device is shared by all handles and threads: calls on
  *    the same device must not overlap in time (issue them on one stream, or
  *    order the streams), otherwise they race on the scratch.
@@ -334,6 +344,22 @@ int mf_matrix_create_transposed(mf_matrix *out, mf_matrix A, void *stream);
  * 1 bypass).  Runs the same device classifier the parity-mode solver uses. */
 int mf_debug_ref_labels(const double *p_old, const double *p_new, int nseg, int *vis,
                         int device_ptrs);
+
+/* Test hook: y = A x with every tile's stored values in one precision:
+ * tile_prec 0 FP64, 1 FP32 (Val_Low), 2 FP16 (round-to-nearest of the FP32
+ * value, the reference encoder's half), 3 INT8 with this library's per-tile
+ * scale.  The stored value is widened to FP64 and multiplied with the FP64 x;
+ * row sums are FP64 in the slice walk's entry order (tile by tile, payload
+ * order within a tile).  Host pointers unless device_ptrs != 0; synchronous.
+ * No counterpart in the reference (its FP16 / INT8 products run only inside
+ * the solver, in half / int8 arithmetic). */
+int mf_debug_spmv_tiles(mf_matrix A, const double *x, double *y, int tile_prec, int device_ptrs);
+
+/* Test hook: the labels the last mf_solve on A in MF_PREC_PARITY left for the
+ * next SpMV's operand p (d_vis codes: 0 FP64, 4 FP32, 3 FP16, 2 INT8, 1
+ * bypass), one per column segment (main-cg-mixed.cu:1323-1370 computes them);
+ * nseg <= max(tilem, tilen).  Undefined after solves in the other precisions. */
+int mf_debug_solver_labels(mf_matrix A, int *vis, int nseg);
 
 /* Library build identity (e.g. "sm_100a"). */
 const char *mf_build_arch(void);

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -92,7 +93,25 @@ void free_matrix(mf_matrix_s *A)
                     A->d_v8, A->d_v8ref, A->d_row_cost};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (A->stage) cudaFree(A->stage);
     delete A;
+}
+
+// Device staging of a host-pointer call (copies of b and x), kept in the handle
+// and grown when a call needs more, so a solve allocates and frees nothing once
+// warm (a stream-ordered allocation per call was returned to the driver at the
+// call's closing synchronisation and mapped again on the next call).
+int stage_get(mf_matrix_s *A, size_t bytes, double **out)
+{
+    if (A->stage_bytes < bytes) {
+        if (A->stage) cudaFree(A->stage);
+        A->stage = nullptr;
+        A->stage_bytes = 0;
+        MF_CUDA_TRY(cudaMalloc(&A->stage, bytes));
+        A->stage_bytes = bytes;
+    }
+    *out = (double *)A->stage;
+    return MF_SUCCESS;
 }
 
 int device_ready()
@@ -175,6 +194,7 @@ extern "C" int mf_matrix_get_info(mf_matrix A, mf_matrix_info *info)
     info->nseg = A->nseg;
     info->slice_entries = A->slice_entries;
     info->build_ms = A->build_ms;
+    info->device = A->dev;
     return MF_SUCCESS;
 }
 
@@ -289,18 +309,25 @@ extern "C" int mf_solve(mf_matrix A, const double *b, double *x, const mf_option
     const double *db = b;
     double *dx = x;
     double *tmp = nullptr;
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
     if (!device_ptrs) {
-        MF_CUDA_TRY(cudaMallocAsync((void **)&tmp, 2 * nb + 16, s));
+        MF_TRY(stage_get(A, 2 * nb + 16, &tmp));
         MF_CUDA_TRY(cudaMemcpyAsync(tmp, b, nb, cudaMemcpyHostToDevice, s));
         db = tmp;
         dx = tmp + A->n_rows;
         if (o.x0_given) MF_CUDA_TRY(cudaMemcpyAsync(dx, x, nb, cudaMemcpyHostToDevice, s));
     }
+    const auto t1 = clk::now();
     int rc = mf_solver_run(A, db, dx, &o, report, s);
+    const auto t2 = clk::now();
     if (!device_ptrs) {
         cudaMemcpyAsync(x, dx, nb, cudaMemcpyDeviceToHost, s);
-        cudaFreeAsync(tmp, s);
         MF_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    if (report) {
+        report->host_ms[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        report->host_ms[3] = std::chrono::duration<double, std::milli>(clk::now() - t2).count();
     }
     return rc;
 }
@@ -322,7 +349,7 @@ extern "C" int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X,
     const double *dB = B;
     double *dX = X, *tmp = nullptr;
     if (!device_ptrs) {
-        MF_CUDA_TRY(cudaMallocAsync((void **)&tmp, 2 * bytes, s));
+        MF_TRY(stage_get(A, 2 * bytes, &tmp));
         MF_CUDA_TRY(cudaMemcpyAsync(tmp, B, bytes, cudaMemcpyHostToDevice, s));
         dB = tmp;
         dX = tmp + (size_t)nrhs * A->n_rows;
@@ -331,7 +358,6 @@ extern "C" int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X,
     int rc = mf_solver_multi_run(A, nrhs, dB, dX, &o, reports, s);
     if (!device_ptrs) {
         cudaMemcpyAsync(X, dX, bytes, cudaMemcpyDeviceToHost, s);
-        cudaFreeAsync(tmp, s);
         MF_CUDA_TRY(cudaStreamSynchronize(s));
     }
     return rc;
@@ -422,7 +448,7 @@ extern "C" int mf_spmv(mf_matrix A, const double *x, double *y, int precision, i
     double *dyp = y;
     double *tmp = nullptr;
     if (!device_ptrs) {
-        MF_CUDA_TRY(cudaMallocAsync((void **)&tmp, ((size_t)A->n_cols + A->n_rows) * sizeof(double) + 16, s));
+        MF_TRY(stage_get(A, ((size_t)A->n_cols + A->n_rows) * sizeof(double) + 16, &tmp));
         MF_CUDA_TRY(cudaMemcpyAsync(tmp, x, (size_t)A->n_cols * sizeof(double), cudaMemcpyHostToDevice, s));
         dxp = tmp;
         dyp = tmp + A->n_cols;
@@ -430,10 +456,35 @@ extern "C" int mf_spmv(mf_matrix A, const double *x, double *y, int precision, i
     int rc = mf_spmv_run(A, dxp, dyp, precision, s, elapsed_ms);
     if (!device_ptrs) {
         cudaMemcpyAsync(y, dyp, (size_t)A->n_rows * sizeof(double), cudaMemcpyDeviceToHost, s);
-        cudaFreeAsync(tmp, s);
         MF_CUDA_TRY(cudaStreamSynchronize(s));
     }
     return rc;
+}
+
+extern "C" int mf_debug_spmv_tiles(mf_matrix A, const double *x, double *y, int tile_prec, int device_ptrs)
+{
+    if (!A || !x || !y || tile_prec < 0 || tile_prec > 3) return MF_ERR_INVALID;
+    const double *dxp = x;
+    double *dyp = y, *tmp = nullptr;
+    if (!device_ptrs) {
+        MF_CUDA_TRY(cudaMalloc((void **)&tmp, ((size_t)A->n_cols + A->n_rows) * sizeof(double) + 16));
+        MF_CUDA_TRY(cudaMemcpy(tmp, x, (size_t)A->n_cols * sizeof(double), cudaMemcpyHostToDevice));
+        dxp = tmp;
+        dyp = tmp + A->n_cols;
+    }
+    // tile_prec 0..3 are the entry precision codes MF_P64, MF_P32, MF_P16, MF_P8
+    int rc = mf_spmv_tiles_run(A, dxp, dyp, tile_prec, 0, nullptr);
+    if (!device_ptrs) {
+        if (rc == MF_SUCCESS) cudaMemcpy(y, dyp, (size_t)A->n_rows * sizeof(double), cudaMemcpyDeviceToHost);
+        cudaFree(tmp);
+    }
+    return rc;
+}
+
+extern "C" int mf_debug_solver_labels(mf_matrix A, int *vis, int nseg)
+{
+    if (!A || (nseg > 0 && !vis)) return MF_ERR_INVALID;
+    return mf_solver_labels_run(A, vis, nseg);
 }
 
 extern "C" int mf_spmv_noalloc(mf_matrix A, const double *x, double *y, int precision, void *stream)

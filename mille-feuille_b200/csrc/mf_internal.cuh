@@ -10,10 +10,15 @@
 //  Solver slices (this library's own format, derived from the tiles):
 //    a tile-row's tiles are cut into segments of <= 15 consecutive tiles; a
 //    segment is a 16-row slice stored as a padded ELL block of Kp columns
-//    (Kp = max row length in the slice rounded up to 8):
-//      meta[off + i*Kp + k]   u8  (slot << 4) | local column   (row-major per row i)
-//      v64/v32/v16/v8[off + k*16 + i]  the entry value in each precision
-//                                         (column-major: 16 lanes read 16 consecutive)
+//    (Kp = max row length in the slice rounded up to 8), i.e. Kp / 8 chunks
+//    of 16 rows x 8 entries (128 entries) back to back.  Within a chunk, row
+//    i's 8 entries are split into 16-byte groups of g = 16 / element size
+//    entries (2 FP64, 4 FP32, 8 FP16 / INT8 / index bytes) and group q of the
+//    16 rows sits together (mf_slot below), so lane i reads its row with one
+//    128-bit load per group and a half-warp's load covers 256 contiguous bytes
+//    (128 for the 8-byte rows of INT8 values and index bytes):
+//      meta[mf_slot<1>(off, k, i)]      u8  (slot << 4) | local column
+//      v64 / v32 / v16 / v8[mf_slot<size>(off, k, i)]  entry k of row i
 //    entries of row i appear tile by tile (slot order), within a tile in the
 //    reference payload order.  Per tile: int8 scale and capability flags.
 #pragma once
@@ -88,10 +93,25 @@ struct mf_matrix_s {
     // cached solver workspace
     void *ws;
     size_t ws_bytes;
+    // device staging of the host-pointer entry points (b / x copies), grow-only
+    void *stage;
+    size_t stage_bytes;
     // tiles exact in INT8 or FP16 (counted on first use; n_exact_known = 0 before)
     int n_exact_known;
     long long n_exact;
 };
+
+// Position of entry k of row i in the slice whose payload starts at entry
+// offset `off` (a multiple of 128), for values of ESZ bytes (8, 4, 2, 1; the
+// index bytes use 1): chunk k / 8, 16-byte group of g = 16 / ESZ entries (at
+// most 8) within the chunk, row i's g entries contiguous inside the group.
+template <int ESZ>
+__host__ __device__ __forceinline__ long long mf_slot(long long off, int k, int i)
+{
+    constexpr int g = ESZ >= 8 ? 2 : ESZ == 4 ? 4 : 8;
+    const int kc = k & 7;
+    return off + (long long)(k >> 3) * 128 + (kc / g) * (16 * g) + i * g + (kc % g);
+}
 
 // ---------------------------------------------------------------- helpers
 
@@ -143,6 +163,9 @@ int mf_batch_schedule_impl(int nitems, const double *cost, const int *tilem, int
                            int *blist, int *queue, int *nqueue);
 int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s,
                 double *elapsed_ms);
+int mf_spmv_tiles_run(mf_matrix_s *A, const double *d_x, double *d_y, int tile_prec, cudaStream_t s,
+                      double *elapsed_ms);
+int mf_solver_labels_run(mf_matrix_s *A, int *vis, int nseg);
 int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s);
 int mf_ref_labels_run(const double *d_pold, const double *d_pnew, int nseg, int *d_vis,
                       cudaStream_t s);

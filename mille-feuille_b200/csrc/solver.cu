@@ -19,6 +19,7 @@
 #include "mf_internal.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -119,7 +120,7 @@ __device__ bool grid_barrier(const SolverParams &P, unsigned &epoch, SH &sh)
 }
 
 // Block partial of up to 4 sums (mask bit k set -> max instead of sum) written
-// to red[kind][block][k].
+// to red[kind][k][block] (value-major, so a collect reads consecutive blocks).
 __device__ void block_partial(const SolverParams &P, Shared &sh, int kind, double v0, double v1, double v2,
                               double v3, int nv, unsigned maxmask)
 {
@@ -147,35 +148,48 @@ __device__ void block_partial(const SolverParams &P, Shared &sh, int kind, doubl
                 double b = __shfl_xor_sync(0xffffffffu, a, o);
                 a = mx ? fmax(a, b) : a + b;
             }
-            if (lane == 0) P.red[((long long)kind * gridDim.x + blockIdx.x) * kRedWidth + k] = a;
+            if (lane == 0) P.red[((long long)kind * kRedWidth + k) * gridDim.x + blockIdx.x] = a;
         }
     }
 }
 
-// After the barrier: every block sums the partials of `kind` in the same order.
+// After the barrier: every block sums the partials of `kind` in the same order
+// (lane c takes blocks c, c + 32, ... in turn, then a shuffle tree).  Partials
+// sit value-major (red[kind][k][block]), warp k reduces value k, and each lane
+// issues all its loads before the first add, so the collect costs one L2 round
+// trip instead of one per partial.  No trailing barrier: the next writer of
+// sh.bcast is the next collect, which every thread reaches only through the
+// barriers of block_partial and grid_barrier, after it has read bcast here.
 __device__ void grid_collect(const SolverParams &P, Shared &sh, int kind, int nv, unsigned maxmask,
                              double *outv)
 {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    if (wib == 0) {
-        for (int k = 0; k < nv; k++) {
-            const bool mx = (maxmask >> k) & 1u;
-            double a = mx ? -1.0e300 : 0.0;
-            for (int c = lane; c < (int)gridDim.x; c += 32) {
-                double b = P.red[((long long)kind * gridDim.x + c) * kRedWidth + k];
-                a = mx ? fmax(a, b) : a + b;
+    if (wib < nv) {
+        const bool mx = (maxmask >> wib) & 1u;
+        const double id = mx ? -1.0e300 : 0.0;
+        const int G = (int)gridDim.x;
+        const double *src = P.red + ((long long)kind * kRedWidth + wib) * G;
+        constexpr int kU = 10;              // 320 blocks per pass: the grid of 148 SMs x 2 in one
+        double a = id;
+        for (int c0 = 0; c0 < G; c0 += 32 * kU) {
+            double t[kU];
+#pragma unroll
+            for (int j = 0; j < kU; j++) {
+                const int cb = c0 + lane + 32 * j;
+                t[j] = cb < G ? src[cb] : id;
             }
 #pragma unroll
-            for (int o = 16; o; o >>= 1) {
-                double b = __shfl_xor_sync(0xffffffffu, a, o);
-                a = mx ? fmax(a, b) : a + b;
-            }
-            if (lane == 0) sh.bcast[k] = a;
+            for (int j = 0; j < kU; j++) a = mx ? fmax(a, t[j]) : a + t[j];
         }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double b = __shfl_xor_sync(0xffffffffu, a, o);
+            a = mx ? fmax(a, b) : a + b;
+        }
+        if (lane == 0) sh.bcast[wib] = a;
     }
     __syncthreads();
     for (int k = 0; k < nv; k++) outv[k] = sh.bcast[k];
-    __syncthreads();
 }
 
 // ------------------------------------------------------------ tile SpMV
@@ -244,6 +258,51 @@ __device__ __forceinline__ int tile_prec(const SolverParams &P, int tw, float st
     return pr;
 }
 
+// Lane i's 8 stored values of the chunk whose payload starts at entry cb (a
+// multiple of 128), in precision PR: 128-bit loads of the row's 16-byte groups
+// (4 for FP64, 2 for FP32, 1 for FP16; an 8-byte load for INT8), each issued
+// only when its first entry lies inside the row (nact entries of the row fall
+// in this chunk; the stored padding past a row's end is zero).  FP32 / FP16 /
+// INT8 values come back as float (INT8 unscaled).
+template <int PR>
+__device__ __forceinline__ void load_chunk(const SolverParams &P, long long cb, int i, int nact,
+                                           double (&v64)[8], float (&v)[8])
+{
+    if (PR == MF_P64) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            double2 d = make_double2(0.0, 0.0);
+            if (2 * q < nact) d = __ldcs((const double2 *)(P.v64 + cb + 32 * q) + i);
+            v64[2 * q] = d.x;
+            v64[2 * q + 1] = d.y;
+        }
+    } else if (PR == MF_P32) {
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (4 * q < nact) f = __ldcs((const float4 *)(P.v32 + cb + 64 * q) + i);
+            v[4 * q] = f.x;
+            v[4 * q + 1] = f.y;
+            v[4 * q + 2] = f.z;
+            v[4 * q + 3] = f.w;
+        }
+    } else if (PR == MF_P16) {
+        uint4 u = make_uint4(0u, 0u, 0u, 0u);
+        if (nact > 0) u = __ldcs((const uint4 *)(P.v16 + cb) + i);
+        const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            v[2 * q] = __half2float(__ushort_as_half((unsigned short)(w[q] & 0xFFFFu)));
+            v[2 * q + 1] = __half2float(__ushort_as_half((unsigned short)(w[q] >> 16)));
+        }
+    } else {
+        uint2 u = make_uint2(0u, 0u);
+        if (nact > 0) u = __ldcs((const uint2 *)(P.v8 + cb) + i);
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = (float)(int8_t)(((j < 4 ? u.x : u.y) >> (8 * (j & 3))) & 0xFFu);
+    }
+}
+
 // Uniform-precision chunk loop: every entry of the slice is stored in
 // precision PR (FP64, FP32, FP16 or scaled INT8); the value is widened to FP64
 // in registers and multiplied with the FP64 x, so the row sum is FP64 and only
@@ -261,50 +320,27 @@ __device__ __forceinline__ double slice_dot_uniform(const SolverParams &P, int4 
                                                     const XVec &X, Pre &pre)
 {
     const int kp = hdr_kp(h);
-    const unsigned long long *mrow = (const unsigned long long *)(P.meta + off + (long long)i * kp);
     float sc = 0.0f;
     if (PR == MF_P8) sc = (i < hdr_nt(h)) ? P.i8_scale[h.x + i] : 0.0f;
     double acc = 0.0;
     for (int k0 = 0; k0 < kp; k0 += 8) {
-        if (PR == MF_P64) {
-            double v[8], xv[8];
+        const long long cb = off + (long long)(k0 >> 3) * 128;
+        double v64[8];
+        float v[8];
+        load_chunk<PR>(P, cb, i, len - k0, v64, v);
+        const unsigned long long m8 = __ldcs((const unsigned long long *)(P.meta + cb) + i);
+        double xv[8];
 #pragma unroll
-            for (int j = 0; j < 8; j++)
-                v[j] = (k0 + j < len) ? __ldcs(P.v64 + off + (long long)(k0 + j) * MF_BS + i) : 0.0;
-            const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
-                const int xi = __shfl_sync(hmask, T.xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
-                xv[j] = (k0 + j < len) ? X.x64[xi] : 0.0;
-            }
-            if (k0 == 0) pre();
-#pragma unroll
-            for (int j = 0; j < 8; j++) acc = fma(v[j], xv[j], acc);
-        } else {
-            float v[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const long long e = off + (long long)(k0 + j) * MF_BS + i;
-                const bool act = k0 + j < len;
-                if (PR == MF_P32) v[j] = act ? __ldcs(P.v32 + e) : 0.0f;
-                else if (PR == MF_P16) v[j] = act ? __half2float(P.v16[e]) : 0.0f;
-                else v[j] = act ? (float)P.v8[e] : 0.0f;
-            }
-            const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
-            double xv[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
-                const int slot = (int)(mm >> 4);
-                const int xi = __shfl_sync(hmask, T.xb, slot, 16) + (int)(mm & 15u);
-                xv[j] = (k0 + j < len) ? X.x64[xi] : 0.0;
-                if (PR == MF_P8) v[j] *= __shfl_sync(hmask, sc, slot, 16);
-            }
-            if (k0 == 0) pre();
-#pragma unroll
-            for (int j = 0; j < 8; j++) acc = fma((double)v[j], xv[j], acc);
+        for (int j = 0; j < 8; j++) {
+            const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+            const int slot = (int)(mm >> 4);
+            const int xi = __shfl_sync(hmask, T.xb, slot, 16) + (int)(mm & 15u);
+            xv[j] = (k0 + j < len) ? X.x64[xi] : 0.0;
+            if (PR == MF_P8) v[j] *= __shfl_sync(hmask, sc, slot, 16);
         }
+        if (k0 == 0) pre();
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc = fma(PR == MF_P64 ? v64[j] : (double)v[j], xv[j], acc);
     }
     return acc;
 }
@@ -363,7 +399,6 @@ __device__ __forceinline__ double slice_dot_parity(const SolverParams &P, int4 h
 {
     const int kp = hdr_kp(h);
     const long long off = hdr_off(h);
-    const unsigned char *mrow = P.meta + off + (long long)i * kp;
     double acc = 0.0;
     double a64[2] = {0.0, 0.0};
     float a32[2] = {0.0f, 0.0f};
@@ -372,7 +407,7 @@ __device__ __forceinline__ double slice_dot_parity(const SolverParams &P, int4 h
     int cur_slot = -1, cur_pr = MF_PSKIP, pos = 0;
     for (int k = 0; k < kp; k++) {
         const bool act = k < len;
-        const unsigned mm = act ? (unsigned)mrow[k] : 0u;
+        const unsigned mm = act ? (unsigned)P.meta[mf_slot<1>(off, k, i)] : 0u;
         const int slot = (int)(mm >> 4);
         const int xi = __shfl_sync(hmask, T.xb, slot, 16) + (int)(mm & 15u);
         const int pr = __shfl_sync(hmask, T.pr, slot, 16);
@@ -387,12 +422,11 @@ __device__ __forceinline__ double slice_dot_parity(const SolverParams &P, int4 h
             cur_pr = pr;
             pos = 0;
         }
-        const long long e = off + (long long)k * MF_BS + i;
         const int q = pos & 1;
-        if (pr == MF_P64) a64[q] = fma(X.x64[xi], P.v64[e], a64[q]);
-        else if (pr == MF_P32) a32[q] = fmaf(X.x32[xi], P.v32[e], a32[q]);
-        else if (pr == MF_P16) a16[q] = __hfma(X.x16[xi], P.v16[e], a16[q]);
-        else if (pr == MF_P8) a8[q] = (int8_t)((int)a8[q] + (int)X.x8[xi] * (int)P.v8ref[e]);
+        if (pr == MF_P64) a64[q] = fma(X.x64[xi], P.v64[mf_slot<8>(off, k, i)], a64[q]);
+        else if (pr == MF_P32) a32[q] = fmaf(X.x32[xi], P.v32[mf_slot<4>(off, k, i)], a32[q]);
+        else if (pr == MF_P16) a16[q] = __hfma(X.x16[xi], P.v16[mf_slot<2>(off, k, i)], a16[q]);
+        else if (pr == MF_P8) a8[q] = (int8_t)((int)a8[q] + (int)X.x8[xi] * (int)P.v8ref[mf_slot<1>(off, k, i)]);
         pos++;
     }
     parity_flush(acc, cur_pr, a64, a32, a16, a8);
@@ -1299,10 +1333,19 @@ __device__ void grid_collect_m(const MultiParams &M, SharedM &sh, int kind, unsi
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     if (wib < NV) {
         const bool mx = (maxmask >> wib) & 1u;
-        double a = mx ? -1.0e300 : 0.0;
-        for (int c = lane; c < nblk; c += 32) {
-            const double b = M.red[((long long)kind * nblk + c) * kRedWidthM + wib];
-            a = mx ? fmax(a, b) : a + b;
+        const double id = mx ? -1.0e300 : 0.0;
+        double a = id;
+        // lane c takes blocks c, c + 32, ...; a pass issues all its loads first
+        constexpr int kU = 5;               // 160 blocks per pass (one block per SM on 148 SMs)
+        for (int c0 = 0; c0 < nblk; c0 += 32 * kU) {
+            double t[kU];
+#pragma unroll
+            for (int j = 0; j < kU; j++) {
+                const int cb = c0 + lane + 32 * j;
+                t[j] = cb < nblk ? M.red[((long long)kind * nblk + cb) * kRedWidthM + wib] : id;
+            }
+#pragma unroll
+            for (int j = 0; j < kU; j++) a = mx ? fmax(a, t[j]) : a + t[j];
         }
 #pragma unroll
         for (int o = 16; o; o >>= 1) {
@@ -1355,53 +1398,36 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
         if (kMixed && pr == MF_P8) sc = (i < hdr_nt(h)) ? P.i8_scale[h.x + i] : 0.0f;
         const int kp = hdr_kp(h);
         const long long off = hdr_off(h);
-        const unsigned long long *mrow = (const unsigned long long *)(P.meta + off + (long long)i * kp);
         for (int k0 = 0; k0 < kp; k0 += 8) {
-            const unsigned long long m8 = __ldcs(mrow + (k0 >> 3));
-            if (!kMixed || pr == MF_P64) {
+            const long long cb = off + (long long)(k0 >> 3) * 128;
+            double v64[8];
+            float vf[8];
+            // stored FP32 / FP16 / scaled-INT8 values are widened to FP64 against
+            // the FP64 operand rows (as the single-column walk): no FP32 copy of R
+            if (!kMixed || pr == MF_P64) load_chunk<MF_P64>(P, cb, i, len - k0, v64, vf);
+            else if (pr == MF_P32) load_chunk<MF_P32>(P, cb, i, len - k0, v64, vf);
+            else if (pr == MF_P16) load_chunk<MF_P16>(P, cb, i, len - k0, v64, vf);
+            else load_chunk<MF_P8>(P, cb, i, len - k0, v64, vf);
+            const unsigned long long m8 = __ldcs((const unsigned long long *)(P.meta + cb) + i);
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
-                    const int xi = __shfl_sync(hmask, xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
-                    if (k0 + j < len) {
-                        const double v = __ldcs(P.v64 + off + (long long)(k0 + j) * MF_BS + i);
-                        if constexpr (NR == 1) {
-                            acc[0] = fma(v, X64[xi], acc[0]);
-                        } else {
-                            const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
+            for (int j = 0; j < 8; j++) {
+                const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+                const int slot = (int)(mm >> 4);
+                const int xi = __shfl_sync(hmask, xb, slot, 16) + (int)(mm & 15u);
+                const float s8 = (kMixed && pr == MF_P8) ? __shfl_sync(hmask, sc, slot, 16) : 0.0f;
+                if (k0 + j < len) {
+                    const double v = (!kMixed || pr == MF_P64) ? v64[j]
+                                     : (pr == MF_P8)           ? (double)(vf[j] * s8)
+                                                               : (double)vf[j];
+                    if constexpr (NR == 1) {
+                        acc[0] = fma(v, X64[xi], acc[0]);
+                    } else {
+                        const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
 #pragma unroll
-                            for (int q = 0; q < NR / 2; q++) {
-                                const double2 d = xr[q];
-                                acc[2 * q] = fma(v, d.x, acc[2 * q]);
-                                acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
-                            }
-                        }
-                    }
-                }
-            } else {
-                // stored FP32 / FP16 / scaled-INT8 values widened to FP64 against the
-                // FP64 operand rows (as the single-column walk): no FP32 copy of R
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
-                    const int slot = (int)(mm >> 4);
-                    const int xi = __shfl_sync(hmask, xb, slot, 16) + (int)(mm & 15u);
-                    const float s8 = (pr == MF_P8) ? __shfl_sync(hmask, sc, slot, 16) : 0.0f;
-                    if (k0 + j < len) {
-                        const long long e = off + (long long)(k0 + j) * MF_BS + i;
-                        const double v = (pr == MF_P32)   ? (double)__ldcs(P.v32 + e)
-                                         : (pr == MF_P16) ? (double)__half2float(P.v16[e])
-                                                          : (double)((float)P.v8[e] * s8);
-                        if constexpr (NR == 1) {
-                            acc[0] = fma(v, X64[xi], acc[0]);
-                        } else {
-                            const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
-#pragma unroll
-                            for (int q = 0; q < NR / 2; q++) {
-                                const double2 d = xr[q];
-                                acc[2 * q] = fma(v, d.x, acc[2 * q]);
-                                acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
-                            }
+                        for (int q = 0; q < NR / 2; q++) {
+                            const double2 d = xr[q];
+                            acc[2 * q] = fma(v, d.x, acc[2 * q]);
+                            acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
                         }
                     }
                 }
@@ -2361,6 +2387,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     const int mode = opt->precision == MF_PREC_FP64 ? MODE_FP64
                      : opt->precision == MF_PREC_PARITY ? MODE_PARITY : MODE_MIXED;
     if (opt->method != MF_METHOD_CG && opt->method != MF_METHOD_BICGSTAB) return MF_ERR_INVALID;
+    const auto t_begin = std::chrono::steady_clock::now();
     Workspace *w = nullptr;
     MF_TRY(ws_get(A, opt->blocks_per_sm, &w, s));
     const long long L = A->vec_len;
@@ -2413,6 +2440,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     // effort; the previous stream attribute and context limit are restored).
     L2Window win;
     if (opt->l2_window) win.set(s, w->vecs, opt->method == MF_METHOD_BICGSTAB ? w->all_bytes : w->cg_bytes);
+    const auto t_prepared = std::chrono::steady_clock::now();
     MF_CUDA_TRY(cudaEventRecord(w->e0, s));
     cudaError_t lerr = cudaLaunchCooperativeKernel(solve_kernel(mode, w->lb), dim3(w->G), dim3(kThreads), args, 0, s);
     if (lerr != cudaSuccess) {
@@ -2431,10 +2459,13 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     MF_CUDA_TRY(cudaMemcpyAsync(d_x, w->x, (size_t)A->n_rows * sizeof(double), cudaMemcpyDeviceToDevice, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
     win.reset(s);
+    const auto t_done = std::chrono::steady_clock::now();
     float ms = 0.f;
     MF_CUDA_TRY(cudaEventElapsedTime(&ms, w->e0, w->e1));
     if (rep) {
         memset(rep, 0, sizeof(*rep));
+        rep->host_ms[1] = std::chrono::duration<double, std::milli>(t_prepared - t_begin).count();
+        rep->host_ms[2] = std::chrono::duration<double, std::milli>(t_done - t_prepared).count();
         rep->iterations = (int)out[0];
         rep->converged = (int)out[1];
         rep->relres_true = out[2];
@@ -2460,8 +2491,11 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     return (int)out[6];
 }
 
-int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s, double *elapsed_ms)
+// y = A x with every tile in one entry precision (MF_P64 .. MF_P8).
+int mf_spmv_tiles_run(mf_matrix_s *A, const double *d_x, double *d_y, int tile_prec, cudaStream_t s,
+                      double *elapsed_ms)
 {
+    if (tile_prec < MF_P64 || tile_prec > MF_P8) return MF_ERR_INVALID;
     // x is read through a padded copy so that column tiles past n_rows read zeros
     Workspace *w = nullptr;
     MF_TRY(ws_get(A, 0, &w, s));
@@ -2474,8 +2508,8 @@ int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, c
     MF_CUDA_TRY(cudaGetDevice(&dev));
     MF_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     // one wave: resident blocks x SMs, each half-warp a contiguous range of tile-rows
-    const int fpr = precision == MF_PREC_FP64 ? MF_P64 : MF_P32;
-    const void *kfn = fpr == MF_P64 ? (const void *)k_spmv<MODE_FP64, 2> : (const void *)k_spmv<MODE_MIXED, 2>;
+    const bool f64 = tile_prec == MF_P64;
+    const void *kfn = f64 ? (const void *)k_spmv<MODE_FP64, 2> : (const void *)k_spmv<MODE_MIXED, 2>;
     int occ = 1;
     MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, kThreads, 0));
     if (occ < 1) occ = 1;
@@ -2486,8 +2520,8 @@ int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, c
     int blocks = (nhw + kWarps * 2 - 1) / (kWarps * 2);
     if (blocks < 1) blocks = 1;
     MF_CUDA_TRY(cudaEventRecord(w->e0, s));
-    if (fpr == MF_P64) k_spmv<MODE_FP64, 2><<<blocks, kThreads, 0, s>>>(P, MF_P64, d_y, rows_per_hw);
-    else k_spmv<MODE_MIXED, 2><<<blocks, kThreads, 0, s>>>(P, MF_P32, d_y, rows_per_hw);
+    if (f64) k_spmv<MODE_FP64, 2><<<blocks, kThreads, 0, s>>>(P, MF_P64, d_y, rows_per_hw);
+    else k_spmv<MODE_MIXED, 2><<<blocks, kThreads, 0, s>>>(P, tile_prec, d_y, rows_per_hw);
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaEventRecord(w->e1, s));
     MF_CUDA_TRY(cudaStreamSynchronize(s));
@@ -2496,6 +2530,23 @@ int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, c
         MF_CUDA_TRY(cudaEventElapsedTime(&ms, w->e0, w->e1));
         *elapsed_ms = ms;
     }
+    return MF_SUCCESS;
+}
+
+int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s, double *elapsed_ms)
+{
+    return mf_spmv_tiles_run(A, d_x, d_y, precision == MF_PREC_FP64 ? MF_P64 : MF_P32, s, elapsed_ms);
+}
+
+// The parity-mode labels the last solve left in the workspace (one per column
+// segment), as d_vis codes.
+int mf_solver_labels_run(mf_matrix_s *A, int *vis, int nseg)
+{
+    Workspace *w = (Workspace *)A->ws;
+    if (!w || nseg < 0 || nseg > std::max(A->tilem, A->tilen)) return MF_ERR_INVALID;
+    std::vector<signed char> h((size_t)nseg + 1);
+    if (nseg > 0) MF_CUDA_TRY(cudaMemcpy(h.data(), w->lab_p, (size_t)nseg, cudaMemcpyDeviceToHost));
+    for (int j = 0; j < nseg; j++) vis[j] = h[j];
     return MF_SUCCESS;
 }
 
@@ -2522,7 +2573,8 @@ std::mutex g_noalloc_mu;
 double *g_noalloc_x_addr[kMaxDevices];
 
 // Device address of the scratch array on the current device, looked up once
-// per device (cudaGetSymbolAddress; the first lookup may load the module).
+// per device (cudaGetSymbolAddress; the first lookup may load the module) and
+// kept while the library stays loaded.
 int noalloc_scratch(int dev, double **x)
 {
     if (dev < 0 || dev >= kMaxDevices) return MF_ERR_UNSUPPORTED;

@@ -492,21 +492,23 @@ __global__ void k_seg_fill(const int *__restrict__ tile_ptr, const int *__restri
                     int st = tptr[cc + i];
                     int sp = (i == rowlen - 1) ? nnzt : (int)tptr[cc + i + 1];
                     for (int e = o + st; e < o + sp; e++) {
-                        meta[off + (long long)i * kp + k] = (unsigned char)(((t - ta) << 4) | tcol[e]);
-                        long long pe = off + (long long)k * MF_BS + i;
-                        v64[pe] = tval[e];
-                        v32[pe] = tval_low[e];
-                        v16[pe] = __float2half_rn(tval_low[e]);
-                        v8[pe] = q8[e];
-                        v8ref[pe] = q8ref[e];
+                        meta[mf_slot<1>(off, k, i)] = (unsigned char)(((t - ta) << 4) | tcol[e]);
+                        v64[mf_slot<8>(off, k, i)] = tval[e];
+                        v32[mf_slot<4>(off, k, i)] = tval_low[e];
+                        v16[mf_slot<2>(off, k, i)] = __float2half_rn(tval_low[e]);
+                        v8[mf_slot<1>(off, k, i)] = q8[e];
+                        v8ref[mf_slot<1>(off, k, i)] = q8ref[e];
                         k++;
                     }
                 }
             }
             for (; k < kp; k++) {
-                meta[off + (long long)i * kp + k] = 0;
-                long long pe = off + (long long)k * MF_BS + i;
-                v64[pe] = 0.0; v32[pe] = 0.0f; v16[pe] = __float2half_rn(0.0f); v8[pe] = 0; v8ref[pe] = 0;
+                meta[mf_slot<1>(off, k, i)] = 0;
+                v64[mf_slot<8>(off, k, i)] = 0.0;
+                v32[mf_slot<4>(off, k, i)] = 0.0f;
+                v16[mf_slot<2>(off, k, i)] = __float2half_rn(0.0f);
+                v8[mf_slot<1>(off, k, i)] = 0;
+                v8ref[mf_slot<1>(off, k, i)] = 0;
             }
         }
     }

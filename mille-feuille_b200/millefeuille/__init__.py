@@ -192,6 +192,23 @@ class Matrix:
         self.last_spmv_ms = ms.value
         return y
 
+    def spmv_tiles(self, x, tile_prec):
+        """Test hook (mf_debug_spmv_tiles): y = A x with every tile stored in
+        one precision -- 0 FP64, 1 FP32, 2 FP16, 3 scaled INT8 -- widened to
+        FP64 against the FP64 x.  Host arrays."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.info["n_rows"], dtype=np.float64)
+        check(_lib.load().mf_debug_spmv_tiles(self._h, _ptr(x), _ptr(y), int(tile_prec), 0), "mf_debug_spmv_tiles")
+        return y
+
+    def solver_labels(self):
+        """Test hook (mf_debug_solver_labels): the labels the last parity-mode
+        solve left for the next SpMV, one per column segment (d_vis codes)."""
+        n = self.info["tilen"]
+        vis = np.zeros(max(n, 1), dtype=np.int32)
+        check(_lib.load().mf_debug_solver_labels(self._h, _ptr(vis), n), "mf_debug_solver_labels")
+        return vis[:n]
+
     def transposed(self, stream=None) -> "Matrix":
         """A handle for A^T (mf_matrix_create_transposed)."""
         L = _lib.load()
@@ -225,14 +242,36 @@ class Matrix:
 
     def spmv_noalloc(self, x, y, precision="fp64", stream=None):
         """y = A x through mf_spmv_noalloc: CUDA tensors only, asynchronous on
-        `stream`, no allocation inside the call (fixed scratch in the library)."""
+        `stream`, no allocation inside the call (fixed scratch in the library).
+
+        The kernel writes n_rows doubles into y and the call copies n_cols
+        doubles out of x without any bounds of its own, so both tensors are
+        checked here before anything is launched: float64, contiguous, at least
+        n_cols / n_rows elements, on the device the matrix was built on.  The
+        call runs with that device current."""
+        import torch
         L = _lib.load()
         if not (_is_cuda_tensor(x) and _is_cuda_tensor(y)):
             raise TypeError("spmv_noalloc takes CUDA tensors for x and y")
-        check(L.mf_spmv_noalloc(self._h, _ptr(x), _ptr(y),
-                                _PREC[precision] if isinstance(precision, str) else precision,
-                                C.c_void_p(stream) if stream else None), "mf_spmv_noalloc")
+        inf = self.info
+        for nm, t, need in (("x", x, inf["n_cols"]), ("y", y, inf["n_rows"])):
+            if t.dtype != torch.float64:
+                raise TypeError(f"spmv_noalloc: {nm} must be float64, got {t.dtype}")
+            if not t.is_contiguous():
+                raise ValueError(f"spmv_noalloc: {nm} must be contiguous")
+            if t.numel() < need:
+                raise ValueError(f"spmv_noalloc: {nm} has {t.numel()} elements, needs {need}")
+        if x.device != y.device:
+            raise ValueError(f"spmv_noalloc: x on {x.device}, y on {y.device}")
+        dev = inf["device"]
+        if x.device.index != dev:
+            raise ValueError(f"spmv_noalloc: tensors on {x.device}, the matrix lives on cuda:{dev}")
+        with torch.cuda.device(dev):
+            check(L.mf_spmv_noalloc(self._h, _ptr(x), _ptr(y),
+                                    _PREC[precision] if isinstance(precision, str) else precision,
+                                    C.c_void_p(stream) if stream else None), "mf_spmv_noalloc")
         return y
+
 
 
 class Batch:

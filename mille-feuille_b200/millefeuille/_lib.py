@@ -36,10 +36,13 @@ class Report(C.Structure):
                 ("relres_true", C.c_double), ("relres_rec", C.c_double), ("residual", C.c_double),
                 ("time_ms", C.c_double), ("replacements", C.c_int), ("grid_blocks", C.c_int),
                 ("threads_per_block", C.c_int), ("tile_uses", C.c_longlong * 4), ("tiles_skipped", C.c_longlong),
-                ("nnz_uses", C.c_longlong * 4), ("phase_ms", C.c_double * 6)]
+                ("nnz_uses", C.c_longlong * 4), ("phase_ms", C.c_double * 6), ("host_ms", C.c_double * 4)]
 
     def as_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("tile_uses", "nnz_uses", "phase_ms")}
+        d = {k: getattr(self, k) for k, _ in self._fields_
+             if k not in ("tile_uses", "nnz_uses", "phase_ms", "host_ms")}
+        d["host_ms"] = dict(zip(("stage_h2d", "prepare", "launch_to_readback", "d2h_sync"),
+                                [round(v, 4) for v in self.host_ms]))
         d["tile_uses"] = list(self.tile_uses)
         d["nnz_uses"] = list(self.nnz_uses)
         d["phase_ms"] = dict(zip(("spmv", "vec_update", "dir_update", "barrier", "replacement", "barrier_spin"),
@@ -51,7 +54,7 @@ class MatrixInfo(C.Structure):
     _fields_ = [("n_rows", C.c_int), ("n_cols", C.c_int), ("nnz", C.c_longlong), ("tilem", C.c_int),
                 ("tilen", C.c_int), ("tilenum", C.c_int), ("csrsize", C.c_int), ("csrptrlen", C.c_int),
                 ("cnt_non_new", C.c_int), ("rowblkblock", C.c_int), ("nseg", C.c_int),
-                ("slice_entries", C.c_longlong), ("build_ms", C.c_double)]
+                ("slice_entries", C.c_longlong), ("build_ms", C.c_double), ("device", C.c_int)]
 
 
 class CgBenchResult(C.Structure):
@@ -66,7 +69,7 @@ EXPORTED = [
     "mf_matrix_destroy", "mf_matrix_get_info", "mf_tile_array_bytes", "mf_tile_export", "mf_solve", "mf_spmv",
     "mf_debug_ref_labels", "mf_build_arch", "mf_spmv_noalloc", "mf_value_grad", "mf_matrix_create_transposed",
     "mf_solve_multi", "mf_batch_create", "mf_batch_tune", "mf_batch_solve", "mf_batch_destroy",
-    "mf_batch_partition", "mf_batch_schedule",
+    "mf_batch_partition", "mf_batch_schedule", "mf_debug_spmv_tiles", "mf_debug_solver_labels",
 ]
 
 _lib = None
@@ -103,6 +106,8 @@ def load() -> C.CDLL:
     L.mf_batch_schedule.argtypes = [C.c_int, dp, ip, C.c_int, ip, ip, ip, ip, ip]
     L.mf_matrix_create_transposed.argtypes = [C.POINTER(vp), vp, vp]
     L.mf_debug_ref_labels.argtypes = [vp, vp, C.c_int, vp, C.c_int]
+    L.mf_debug_spmv_tiles.argtypes = [vp, vp, vp, C.c_int, C.c_int]
+    L.mf_debug_solver_labels.argtypes = [vp, vp, C.c_int]
     L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
     L.mf_write_cbd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp]
     L.mf_free_host.argtypes = [vp]

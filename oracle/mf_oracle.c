@@ -24,6 +24,9 @@
 
 #define BS 16
 
+static size_t vec_len(const orc_tiles *T, int n);
+static void spmv_tile_exact(const orc_tiles *T, int rowA, const double *x, double *y, int nthreads);
+
 void orc_free(void *p) { free(p); }
 
 static int cmp_int(const void *a, const void *b)
@@ -380,6 +383,70 @@ float orc_f16_to_f32(uint16_t h)
     return f;
 }
 
+/* binary64 -> binary16, round to nearest even, of the exact value s + e where
+ * |e| is below half an ulp of s (TwoSum's error term; 0 for a plain double).
+ * Written from the IEEE 754 definition: the dropped bits of s decide the
+ * rounding, and only when they sit exactly on the halfway point does e (its
+ * sign relative to s) break the tie; e = 0 breaks it to even. */
+uint16_t orc_f64_to_f16_rn(double s, double e)
+{
+    uint64_t u;
+    memcpy(&u, &s, 8);
+    uint16_t sign = (uint16_t)((u >> 48) & 0x8000u);
+    int ex = (int)((u >> 52) & 0x7FF);
+    uint64_t man = u & 0xFFFFFFFFFFFFFull;
+    if (ex == 0x7FF) {                          /* inf / nan */
+        if (man == 0) return (uint16_t)(sign | 0x7C00u);
+        return (uint16_t)(sign | 0x7E00u | (uint16_t)(man >> 42));
+    }
+    if (ex == 0) return sign;                   /* zero or double subnormal: far below half's range */
+    int eh = ex - 1023 + 15;
+    if (eh >= 31) return (uint16_t)(sign | 0x7C00u);   /* |s| >= 2^16: overflow */
+    uint64_t q, rem, half;
+    if (eh <= 0) {                              /* half subnormal: units of 2^-24 */
+        int shift = 1051 - ex;                  /* m * 2^(ex - 1075) / 2^-24 */
+        if (shift >= 54) return sign;           /* below a quarter of the smallest subnormal */
+        uint64_t m = man | (1ull << 52);
+        q = m >> shift;
+        rem = m & ((1ull << shift) - 1);
+        half = 1ull << (shift - 1);
+    } else {
+        q = ((uint64_t)eh << 10) | (man >> 42);
+        rem = man & ((1ull << 42) - 1);
+        half = 1ull << 41;
+    }
+    int up;
+    if (rem != half) up = rem > half;
+    else if (e != 0.0) up = (e > 0.0) == (s > 0.0);   /* e moves the magnitude off the tie */
+    else up = (int)(q & 1u);
+    if (up) q++;                                /* a carry into the exponent is the correct result */
+    return (uint16_t)(sign | (uint16_t)q);
+}
+
+/* __hfma(a, b, c): a * b + c rounded once to binary16.  The product of two
+ * 11-bit significands is exact in binary64, the sum is split into s + e by
+ * TwoSum (Knuth), and s + e is rounded to binary16 in one step. */
+uint16_t orc_hfma(uint16_t a, uint16_t b, uint16_t c)
+{
+    const double fa = orc_f16_to_f32(a), fb = orc_f16_to_f32(b), fc = orc_f16_to_f32(c);
+    const double p = fa * fb;
+    const double sm = p + fc;
+    if (sm != sm || sm == INFINITY || sm == -INFINITY) return orc_f64_to_f16_rn(sm, 0.0);
+    const double bv = sm - p;
+    const double err = (p - (sm - bv)) + (fc - bv);
+    return orc_f64_to_f16_rn(sm, err);
+}
+
+/* (int8_t) of a double as the x86-64 host compiler emits it: truncate to
+ * int32 (0x80000000 when NaN or out of range), keep the low byte. */
+static int8_t trunc_i8(double v)
+{
+    int32_t w;
+    if (v != v || v >= 2147483648.0 || v < -2147483648.0) w = (int32_t)0x80000000u;
+    else w = (int32_t)v;
+    return (int8_t)(uint8_t)(w & 0xFF);
+}
+
 /* Encoder (main-cg-mixed.cu:2333-2350): half = RN(float value) (the float copy
  * is itself RN(double)); int8 = C truncation of the double.  The reference's
  * out-of-range int8 conversion is undefined in C; this restates what the x86-64
@@ -389,11 +456,7 @@ void orc_encode_ref(int n, const double *val, const float *val_low,
 {
     for (int i = 0; i < n; i++) {
         val_f16[i] = orc_f32_to_f16_rn(val_low[i]);
-        double v = val[i];
-        int32_t w;
-        if (v != v || v >= 2147483648.0 || v < -2147483648.0) w = (int32_t)0x80000000u;
-        else w = (int32_t)v;
-        val_i8[i] = (int8_t)(uint8_t)(w & 0xFF);
+        val_i8[i] = trunc_i8(val[i]);
     }
 }
 
@@ -501,6 +564,192 @@ static void spmv_tile_exact(const orc_tiles *T, int rowA, const double *x, doubl
         }
         for (int ri = 0; ri < rl; ri++) y[(size_t)R * BS + ri] = acc[ri];
     }
+}
+
+/* The stored value of entry e of tile t in precision prec, widened to FP64. */
+static double stored_value(const orc_tiles *T, int t, int e, int prec, const uint16_t *v16, const int8_t *q8,
+                           const float *scale)
+{
+    switch (prec) {
+    case 0: return T->val[e];
+    case 1: return (double)T->val_low[e];
+    case 2: return (double)orc_f16_to_f32(v16[e]);
+    default: return (double)((float)q8[e] * scale[t]);
+    }
+}
+
+/* The product of the encoded values (the values the reference's tile SpMV,
+ * main-cg-mixed.cu:1130-1214, multiplies in each precision; INT8 with the
+ * per-tile scale of this build), accumulated in FP64 in the GPU slice walk's
+ * order: per row, tile by tile in slices of 15, payload order within a tile. */
+void orc_spmv_slices(const orc_tiles *T, int rowA, const double *x, double *y, int prec,
+                     const uint16_t *v16, const int8_t *q8, const float *scale)
+{
+    for (int R = 0; R < T->tilem; R++) {
+        const int rl = (R == T->tilem - 1) ? rowA - R * BS : BS;
+        const int t0 = T->tile_ptr[R], t1 = T->tile_ptr[R + 1];
+        for (int ri = 0; ri < rl; ri++) {
+            double acc = 0.0;
+            for (int ts = t0; ts < t1; ts += 15) {
+                const int te = (ts + 15 < t1) ? ts + 15 : t1;
+                double sacc = 0.0;
+                for (int t = ts; t < te; t++) {
+                    const double *xo = x + (size_t)T->tile_columnidx[t] * BS;
+                    const int off = T->csr_offset[t], nz = T->csr_offset[t + 1] - off;
+                    const unsigned char *pt = T->ptr + T->csrptr_offset[t];
+                    const int st = pt[ri], sp = (ri == rl - 1) ? nz : pt[ri + 1];
+                    for (int k = st; k < sp; k++)
+                        sacc = fma(stored_value(T, t, off + k, prec, v16, q8, scale), xo[T->col[off + k]], sacc);
+                }
+                acc += sacc;
+            }
+            y[(size_t)R * BS + ri] = acc;
+        }
+    }
+}
+
+/* Tile products of the reference's mixed SpMV (main-cg-mixed.cu:1130-1214):
+ * per (tile, row) two partial sums, entries at even / odd positions of the
+ * row (the reference's lane pair, virtual_lane_id), in the precision of the
+ * column segment's label -- FP64 fma on p, FP32 fmaf on (float)p, FP16 __hfma
+ * on half(p), INT8 int8 sums (wrapping) of (int8_t)p times the truncated
+ * values, bypass skipped -- each partial widened and added to the row's FP64
+ * sum, even then odd, tile by tile.  The reference adds them with atomics in
+ * no fixed order; this is the fixed order of the GPU parity mode (per slice of
+ * 15 tiles, slice sums added in turn). */
+static void spmv_parity(const orc_tiles *T, int rowA, const double *p, const float *p32, const uint16_t *p16,
+                        const int8_t *p8, const int *lab, const uint16_t *v16, const int8_t *i8ref, double *y)
+{
+    for (int R = 0; R < T->tilem; R++) {
+        const int rl = (R == T->tilem - 1) ? rowA - R * BS : BS;
+        const int t0 = T->tile_ptr[R], t1 = T->tile_ptr[R + 1];
+        for (int ri = 0; ri < rl; ri++) {
+            double acc = 0.0;
+            for (int ts = t0; ts < t1; ts += 15) {
+                const int te = (ts + 15 < t1) ? ts + 15 : t1;
+                double sacc = 0.0;
+                for (int t = ts; t < te; t++) {
+                    const int j = T->tile_columnidx[t];
+                    const int code = lab[j];
+                    const int off = T->csr_offset[t], nz = T->csr_offset[t + 1] - off;
+                    const unsigned char *pt = T->ptr + T->csrptr_offset[t];
+                    const int st = pt[ri], sp = (ri == rl - 1) ? nz : pt[ri + 1];
+                    if (code == 1 || st >= sp) continue;
+                    double a64[2] = {0.0, 0.0};
+                    float a32[2] = {0.0f, 0.0f};
+                    uint16_t a16[2] = {0, 0};
+                    int8_t a8[2] = {0, 0};
+                    for (int k = st; k < sp; k++) {
+                        const int e = off + k, q = (k - st) & 1;
+                        const size_t col = (size_t)j * BS + T->col[e];
+                        if (code == 0) a64[q] = fma(p[col], T->val[e], a64[q]);
+                        else if (code == 4) a32[q] = fmaf(p32[col], T->val_low[e], a32[q]);
+                        else if (code == 3) a16[q] = orc_hfma(p16[col], v16[e], a16[q]);
+                        else a8[q] = (int8_t)((int)a8[q] + (int)p8[col] * (int)i8ref[e]);
+                    }
+                    for (int q = 0; q < 2; q++) {
+                        if (code == 0) sacc += a64[q];
+                        else if (code == 4) sacc += (double)a32[q];
+                        else if (code == 3) sacc += (double)orc_f16_to_f32(a16[q]);
+                        else sacc += (double)a8[q];
+                    }
+                }
+                acc += sacc;
+            }
+            y[(size_t)R * BS + ri] = acc;
+        }
+    }
+}
+
+static double dot_seq(int n, const double *a, const double *b)
+{
+    double t = 0.0;
+    for (int i = 0; i < n; i++) t += a[i] * b[i];
+    return t;
+}
+
+/* Parity-mode CG (main-cg-mixed.cu:1115-1385), the reference's three phases
+ * per iteration: q = A p with the label-selected tile arithmetic, alpha =
+ * r.r / p.q, r -= alpha q, beta = r'.r' / r.r, x += alpha p, p = r + beta p;
+ * then p's shadows (float)p, half(p) (__double2half, one rounding) and
+ * (int8_t)p (the int8 conversion of main-cg-mixed.cu:434) and the labels of
+ * the next SpMV from |p_new - p_old| per 16-element segment (thresholds of
+ * main-cg-mixed.cu:1334-1351).  The reference keeps the class of whichever
+ * lane wrote last; here the most conservative class wins (one of the
+ * reference's possible outcomes) and agree[s] says whether every lane of the
+ * segment had the same class (the reference's label is then determined).
+ * x0 = 0, labels start all FP64 (cudaMemset(d_vis, 0), main-cg-mixed.cu:2828).
+ * Dot products are sequential sums.  The axpys use fma as nvcc contracts
+ * them. */
+int orc_cg_parity(const orc_tiles *T, int n, const double *b, const uint16_t *v16, const int8_t *i8ref,
+                  double *x, int iters, int *labels, int *agree, orc_report *rep)
+{
+    const size_t N = vec_len(T, n);
+    const int nseg = (int)(N / BS);
+    double *r = (double *)calloc(N, sizeof(double));
+    double *p = (double *)calloc(N, sizeof(double));
+    double *q = (double *)calloc(N, sizeof(double));
+    double *xx = (double *)calloc(N, sizeof(double));
+    double *pold = (double *)calloc(N, sizeof(double));
+    float *p32 = (float *)calloc(N, sizeof(float));
+    uint16_t *p16 = (uint16_t *)calloc(N, sizeof(uint16_t));
+    int8_t *p8 = (int8_t *)calloc(N, sizeof(int8_t));
+    int *lab = (int *)calloc((size_t)nseg, sizeof(int));
+    int *agr = (int *)calloc((size_t)nseg, sizeof(int));
+    for (int i = 0; i < n; i++) {
+        r[i] = b[i];
+        p[i] = b[i];
+        p32[i] = (float)b[i];
+        p16[i] = orc_f64_to_f16_rn(b[i], 0.0);
+        p8[i] = trunc_i8(b[i]);
+    }
+    for (int s = 0; s < nseg; s++) agr[s] = 1;
+    double rr = dot_seq(n, r, r);
+    const double bb = rr;
+    for (int k = 0; k < iters; k++) {
+        spmv_parity(T, n, p, p32, p16, p8, lab, v16, i8ref, q);
+        const double alpha = rr / dot_seq(n, p, q);
+        for (int i = 0; i < n; i++) r[i] = fma(-alpha, q[i], r[i]);
+        const double rr_new = dot_seq(n, r, r);
+        const double beta = rr_new / rr;
+        rr = rr_new;
+        memcpy(pold, p, N * sizeof(double));
+        for (int i = 0; i < n; i++) {
+            xx[i] = fma(alpha, pold[i], xx[i]);
+            p[i] = fma(beta, pold[i], r[i]);
+            p32[i] = (float)p[i];
+            p16[i] = orc_f64_to_f16_rn(p[i], 0.0);
+            p8[i] = trunc_i8(p[i]);
+        }
+        for (int s = 0; s < nseg; s++) {
+            int rank = 0, c0 = -1, same = 1;
+            for (int i = s * BS; i < s * BS + BS && i < n; i++) {
+                const int c = orc_classify_ref(fabs(p[i] - pold[i]));
+                const int rk = (c == 1) ? 4 : (c == 4) ? 3 : (c == 3) ? 2 : (c == 2) ? 1 : 0;
+                if (rk > rank) rank = rk;
+                if (c0 < 0) c0 = c;
+                else if (c != c0) same = 0;
+            }
+            static const int code[5] = {1, 2, 3, 4, 0};
+            lab[s] = code[rank];
+            agr[s] = same;
+        }
+    }
+    spmv_tile_exact(T, n, xx, q, 1);
+    double rt = 0.0;
+    for (int i = 0; i < n; i++) { const double d = b[i] - q[i]; rt += d * d; }
+    memcpy(x, xx, (size_t)n * sizeof(double));
+    if (labels) memcpy(labels, lab, (size_t)T->tilen * sizeof(int));
+    if (agree) memcpy(agree, agr, (size_t)T->tilen * sizeof(int));
+    if (rep) {
+        rep->iterations = iters;
+        rep->converged = 0;
+        rep->relres_rec = bb > 0 ? sqrt(rr / bb) : 0.0;
+        rep->relres_true = bb > 0 ? sqrt(rt / bb) : 0.0;
+        rep->replacements = 0;
+    }
+    free(r); free(p); free(q); free(xx); free(pold); free(p32); free(p16); free(p8); free(lab); free(agr);
+    return 0;
 }
 
 void orc_csr_spmv(int n, const int *rowptr, const int *colidx, const double *val,

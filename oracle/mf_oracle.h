@@ -108,6 +108,32 @@ int orc_bicgstab_fp64(const orc_tiles *T, const orc_rowlists *L, int n,
                       const double *b, double *x, double tol, int max_iter,
                       int fixed_iters, int nthreads, orc_report *rep);
 
+/* binary64 value s + e (|e| below half an ulp of s, e.g. TwoSum's error
+ * term) -> binary16, round to nearest, ties to even, with e deciding a tie of
+ * s alone.  e = 0: the conversion __double2half performs. */
+uint16_t orc_f64_to_f16_rn(double s, double e);
+/* a * b + c rounded once to binary16 (the semantics of CUDA's __hfma). */
+uint16_t orc_hfma(uint16_t a, uint16_t b, uint16_t c);
+
+/* y = A x with every tile's values in one stored precision, in the order the
+ * GPU slice walk accumulates: per row, the entries tile by tile in payload
+ * order, fma-folded into an FP64 sum that starts at 0 for each slice of
+ * <= 15 consecutive tiles; the slice sums are added in turn.  prec: 0 FP64
+ * values, 1 FP32 (val_low), 2 FP16 (v16 bits, RN of val_low), 3 scaled INT8
+ * (q8 times the tile's float scale, product in float).  The stored value is
+ * widened to FP64 and multiplied with the FP64 x. */
+void orc_spmv_slices(const orc_tiles *T, int rowA, const double *x, double *y, int prec,
+                     const uint16_t *v16, const int8_t *q8, const float *scale);
+
+/* Parity-mode CG: the reference's mixed single-kernel CG
+ * (main-cg-mixed.cu:1115-1385) on `iters` fixed iterations from x0 = 0, with
+ * the labels of the next SpMV in *labels (tilen codes: 0 FP64, 4 FP32, 3 FP16,
+ * 2 INT8, 1 bypass) and, per segment, whether every lane's class agreed
+ * (agree, nullable).  v16 / i8ref: the reference encoder's FP16 and truncated
+ * INT8 values (orc_encode_ref). */
+int orc_cg_parity(const orc_tiles *T, int n, const double *b, const uint16_t *v16, const int8_t *i8ref,
+                  double *x, int iters, int *labels, int *agree, orc_report *rep);
+
 /* CSR SpMV y = A x over rows [0,n) (Mille-feuille-bicg.h:31-41 `mv`). */
 void orc_csr_spmv(int n, const int *rowptr, const int *colidx, const double *val,
                   const double *x, double *y, int nthreads);

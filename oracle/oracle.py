@@ -80,6 +80,13 @@ def _load():
                                  C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.POINTER(C.c_int)),
                                  C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_int)]
     lib.orc_free.argtypes = [C.c_void_p]
+    lib.orc_f64_to_f16_rn.argtypes = [C.c_double, C.c_double]
+    lib.orc_f64_to_f16_rn.restype = C.c_uint16
+    lib.orc_hfma.argtypes = [C.c_uint16, C.c_uint16, C.c_uint16]
+    lib.orc_hfma.restype = C.c_uint16
+    lib.orc_spmv_slices.argtypes = [C.POINTER(OrcTiles), C.c_int, _f64p, _f64p, C.c_int, _u16p, _i8p, _f32p]
+    lib.orc_cg_parity.argtypes = [C.POINTER(OrcTiles), C.c_int, _f64p, _u16p, _i8p, _f64p, C.c_int, _i32p, _i32p,
+                                  C.POINTER(OrcReport)]
     return lib
 
 
@@ -184,6 +191,46 @@ class Tiles:
                        relres_rec=rep.relres_rec, relres_true=rep.relres_true,
                        replacements=rep.replacements)
 
+    def _encoded(self):
+        """The reference encoder's FP16 / truncated INT8 values and this
+        build's scaled INT8 values, in tile payload order (cached)."""
+        if not hasattr(self, "_enc"):
+            a = self.arrays()
+            f16, i8ref = encode_ref(a["val"], a["val_low"])
+            q8, sc = encode_i8_scaled(self)
+            pad = lambda v, dt: np.ascontiguousarray(v if v.size else np.zeros(1, dt), dtype=dt)
+            self._enc = (pad(f16, np.uint16), pad(i8ref, np.int8), pad(q8, np.int8), pad(sc, np.float32))
+        return self._enc
+
+    def spmv_slices(self, x, prec):
+        """y = A x with every tile's values stored in one precision (0 FP64,
+        1 FP32, 2 FP16, 3 scaled INT8), FP64 accumulation in the GPU slice
+        walk's entry order (orc_spmv_slices)."""
+        f16, _, q8, sc = self._encoded()
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        need = max(self.t.tilen * 16, self.rowA)
+        if x.size < need:
+            x = np.concatenate([x, np.zeros(need - x.size)])
+        y = np.zeros(max(self.t.tilem * 16, self.rowA, 1), dtype=np.float64)
+        lib().orc_spmv_slices(C.byref(self.t), self.rowA, x, y, int(prec), f16, q8, sc)
+        return y[: self.rowA]
+
+    def cg_parity(self, b, iters):
+        """The reference's mixed CG (parity arithmetic and label rule) for
+        `iters` fixed iterations from x0 = 0 (orc_cg_parity).  Returns (x,
+        labels of the next SpMV per column segment, all-lanes-agree mask,
+        report)."""
+        f16, i8ref, _, _ = self._encoded()
+        b = np.ascontiguousarray(b[: self.rowA], dtype=np.float64)
+        x = np.zeros(self.rowA, dtype=np.float64)
+        nseg = max(self.t.tilen, 1)
+        labels = np.zeros(nseg, dtype=np.int32)
+        agree = np.zeros(nseg, dtype=np.int32)
+        rep = OrcReport()
+        lib().orc_cg_parity(C.byref(self.t), self.rowA, b, f16, i8ref, x, int(iters), labels, agree, C.byref(rep))
+        return x, labels[: self.t.tilen], agree[: self.t.tilen].astype(bool), dict(
+            iterations=rep.iterations, relres_rec=rep.relres_rec, relres_true=rep.relres_true)
+
     def cg_fp64(self, b, tol=1e-8, max_iter=10000, fixed_iters=False, nthreads=1):
         return self._solve(lib().orc_cg_fp64, b, tol, max_iter, fixed_iters, nthreads)
 
@@ -207,6 +254,15 @@ def encode_i8_scaled(tiles: Tiles):
     s = np.zeros(max(tiles.t.tilenum, 1), dtype=np.float32)
     lib().orc_encode_i8_scaled(C.byref(tiles.t), q, s)
     return q[: tiles.t.csrsize], s[: tiles.t.tilenum]
+
+
+def f64_to_f16_rn(s, e=0.0):
+    return int(lib().orc_f64_to_f16_rn(float(s), float(e)))
+
+
+def hfma(a, b, c):
+    """__hfma on binary16 bit patterns (orc_hfma)."""
+    return int(lib().orc_hfma(int(a), int(b), int(c)))
 
 
 def segment_labels_ref(p_old, p_new):

@@ -198,3 +198,77 @@ def test_aniso2d_grf_generator():
     assert S[65, 129] == pytest.approx(-hm(kap[1, 1], kap[2, 1]), rel=1e-14)
     A2, B2, _, _ = M.aniso2d_grf(64, seed=4, corr=16.0, nrhs=3)
     assert np.array_equal(A2.val, A.val) and np.array_equal(B2, B)
+
+
+def test_oracle_f64_to_f16_and_hfma(oracle_mod):
+    """The oracle's binary16 conversion matches numpy's (round to nearest even
+    from binary64, overflow to inf, subnormals); __hfma's single rounding is
+    checked against the exact rational a*b + c rounded to the nearest half."""
+    from fractions import Fraction
+    rng = np.random.default_rng(0)
+    v = np.concatenate([rng.standard_normal(20000) * 10.0 ** rng.integers(-9, 6, 20000),
+                        [65504.0, 65519.99, 65520.0, 6e-8, 2.98e-8, 2.0 ** -25, -0.0, 0.0, np.inf, -np.inf]])
+    with np.errstate(over="ignore"):
+        ref = v.astype(np.float16).view(np.uint16)
+    got = np.array([oracle_mod.f64_to_f16_rn(t) for t in v], dtype=np.uint16)
+    np.testing.assert_array_equal(got, ref)
+    # a tie of s alone broken by the error term: 1 + 2^-11 is halfway between 1 and 1 + 2^-10
+    s = 1.0 + 2.0 ** -11
+    assert oracle_mod.f64_to_f16_rn(s, 0.0) == 0x3C00             # ties to even -> 1.0
+    assert oracle_mod.f64_to_f16_rn(s, 2.0 ** -60) == 0x3C01      # just above the tie
+    assert oracle_mod.f64_to_f16_rn(-s, -(2.0 ** -60)) == 0xBC01  # magnitude above the tie
+
+    def h2f(h):
+        return Fraction(float(np.array([h], dtype=np.uint16).view(np.float16)[0]))
+
+    def nearest(fr):
+        f = float(fr)
+        base = int(np.array([np.float16(f)]).view(np.uint16)[0])
+        best = None
+        for d in (-2, -1, 0, 1, 2):
+            c = (base + d) & 0xFFFF
+            val = np.array([c], dtype=np.uint16).view(np.float16)[0]
+            if not np.isfinite(val):
+                continue
+            key = (abs(Fraction(float(val)) - fr), c & 1)
+            if best is None or key < best[0]:
+                best = (key, c)
+        return best[1]
+
+    for _ in range(3000):
+        a, b, c = (np.float16(rng.standard_normal() * 10.0 ** rng.integers(-4, 3)) for _ in range(3))
+        ha, hb, hc = (int(np.array([t]).view(np.uint16)[0]) for t in (a, b, c))
+        exact = h2f(ha) * h2f(hb) + h2f(hc)
+        if exact == 0 or abs(float(exact)) > 60000:
+            continue
+        assert oracle_mod.hfma(ha, hb, hc) == nearest(exact)
+
+
+def test_oracle_spmv_slices_and_parity_cg(oracle_mod):
+    """The slice-order product of the encoded values agrees with the FP64 CSR
+    product within each encoding's rounding; with every label FP64 (b of unit
+    size, so |p_new - p_old| > 1e-5 everywhere) the parity-mode CG is the FP64
+    CG of the same schedule."""
+    from millefeuille import matrices as M
+    A = M.random_csr(200, 230, 0.08, seed=4)
+    T = oracle_mod.Tiles(A.n, 230, A.rowptr, A.colidx, A.val)
+    x = np.random.default_rng(1).uniform(-1, 1, 230)
+    import scipy.sparse as sp
+    S = sp.csr_matrix((A.val, A.colidx, A.rowptr), shape=(A.n, 230))
+    ye, sc = S @ x, abs(S) @ np.abs(x)
+    for prec, rel in ((0, 1e-14), (1, 1.2e-7), (2, 1e-3)):
+        assert np.all(np.abs(T.spmv_slices(x, prec) - ye) <= rel * sc)
+    A2, b2, _ = M.laplace2d_system(24, seed=0)
+    T2 = oracle_mod.Tiles(A2.n, A2.n, A2.rowptr, A2.colidx, A2.val)
+    for k in (1, 5, 12):
+        xp, lab, agree, rp = T2.cg_parity(b2, k)
+        xf, rf = T2.cg_fp64(b2, max_iter=k, fixed_iters=True)
+        assert np.all(lab == 0)
+        np.testing.assert_allclose(xp, xf, rtol=1e-10, atol=1e-12 * np.abs(xf).max())
+        assert rp["relres_true"] == pytest.approx(rf["relres_true"], rel=1e-8)
+    # scaled right-hand side: labels spread over the reduced classes, deterministically
+    xa, la, _, _ = T2.cg_parity(b2 * 2e-6, 20)
+    xb, lb, _, _ = T2.cg_parity(b2 * 2e-6, 20)
+    np.testing.assert_array_equal(la, lb)
+    np.testing.assert_array_equal(xa, xb)
+    assert set(la.tolist()) >= {2, 3}
