@@ -52,7 +52,12 @@ typedef struct {
 
 /*
  * Replaces cg_solve_inc of main-cg-mixed.cu:2248 (mixed-precision single
- * kernel).  Same arguments and meaning: n is the row count already truncated
+ * kernel) in libmillefeuille.so, and cg_solve_inc of main-cg.cu:1110 (FP64;
+ * main-cg calls it for nnz < 10,000, main-cg.cu:1727-1745) in
+ * libmillefeuille_fp64.so, which is otherwise the same library: link the
+ * library that matches the reference driver being replaced (mf_build_arch
+ * names the variant; the FP64 one writes cg_performance.csv).
+ * Same arguments and meaning: n is the row count already truncated
  * to a multiple of 16 by the caller, ori the original column count, x is
  * zeroed and returned, exactly max_iter iterations are run (the reference has
  * no convergence exit); iter, maxiter and threshold are ignored as in the
@@ -360,6 +365,12 @@ int mf_debug_spmv_tiles(mf_matrix A, const double *x, double *y, int tile_prec, 
  * bypass), one per column segment (main-cg-mixed.cu:1323-1370 computes them);
  * nseg <= max(tilem, tilen).  Undefined after solves in the other precisions. */
 int mf_debug_solver_labels(mf_matrix A, int *vis, int nseg);
+
+/* Test hook: the full report (mf_report) of the calling thread's last
+ * drop-in solve (cg_solve_inc / _sync / _reduce, bicgstab / _sync / _inc), so a
+ * caller of the reference's entry points can see which precision ran
+ * (tile_uses).  No counterpart in the reference. */
+int mf_dropin_last_report(mf_report *out);
 
 /* Library build identity (e.g. "sm_100a"). */
 const char *mf_build_arch(void);

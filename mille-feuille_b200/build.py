@@ -2,10 +2,13 @@
 
     python mille-feuille_b200/build.py [--verbose]
 
-Object files go to mille-feuille_b200/_build/, the shared library to
-mille-feuille_b200/millefeuille/libmillefeuille.so and the drop-in driver
-executables (main-cg, main-cg-mixed, main-bicg, main-bicg-mixed) to
-mille-feuille_b200/bin/ (all git-ignored, carried with the tree).  Rebuilds
+Object files go to mille-feuille_b200/_build/, the shared libraries to
+mille-feuille_b200/millefeuille/: libmillefeuille.so (cg_solve_inc is the
+mixed-precision solver of main-cg-mixed.cu) and libmillefeuille_fp64.so (the
+same objects with api.cu built with MF_CG_INC_FP64: cg_solve_inc is the FP64
+solver of main-cg.cu).  The drop-in driver executables (main-cg, main-cg-mixed,
+main-bicg, main-bicg-mixed) go to mille-feuille_b200/bin/, main-cg linked
+against the FP64 variant (all git-ignored, carried with the tree).  Rebuilds
 only what changed.
 """
 from __future__ import annotations
@@ -18,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "millefeuille", "libmillefeuille.so")
+OUT_FP64 = os.path.join(HERE, "millefeuille", "libmillefeuille_fp64.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -35,32 +39,42 @@ def _newer(src: str, dst: str, deps) -> bool:
     return any(os.path.getmtime(p) > t for p in [src, *deps])
 
 
+def _compile(src: str, obj: str, deps, verbose: bool, defines=()) -> None:
+    if not _newer(src, obj, deps):
+        return
+    cmd = [NVCC, *ARCH, *CUFLAGS, *[f"-D{d}" for d in defines], "-c", src, "-o", obj]
+    if verbose and src.endswith(".cu"):
+        cmd += ["-Xptxas", "-v"]
+    if src.endswith(".cpp"):
+        cmd = ["g++", "-O2", "-fPIC", "-pthread", "-std=c++17", "-I", INCLUDE, "-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or r.returncode:
+        sys.stderr.write(r.stdout + r.stderr)
+    if r.returncode:
+        raise RuntimeError(f"compile failed: {os.path.basename(src)}")
+
+
+def _link(out: str, objs) -> None:
+    if any(_newer(o, out, []) for o in objs) or not os.path.exists(out):
+        cmd = [NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart", "-Xcompiler", "-pthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"link failed: {os.path.basename(out)}")
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     deps = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "millefeuille.h")]
     objs = []
     for src in SOURCES:
-        sp = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
         objs.append(obj)
-        if not _newer(sp, obj, deps):
-            continue
-        cmd = [NVCC, *ARCH, *CUFLAGS, "-c", sp, "-o", obj]
-        if verbose and src.endswith(".cu"):
-            cmd += ["-Xptxas", "-v"]
-        if src.endswith(".cpp"):
-            cmd = ["g++", "-O2", "-fPIC", "-pthread", "-std=c++17", "-I", INCLUDE, "-c", sp, "-o", obj]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if verbose or r.returncode:
-            sys.stderr.write(r.stdout + r.stderr)
-        if r.returncode:
-            raise RuntimeError(f"compile failed: {src}")
-    if any(_newer(o, OUT, []) for o in objs) or not os.path.exists(OUT):
-        cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart", "-Xcompiler", "-pthread"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if r.returncode:
-            sys.stderr.write(r.stdout + r.stderr)
-            raise RuntimeError("link failed")
+        _compile(os.path.join(CSRC, src), obj, deps, verbose)
+    api_fp64 = os.path.join(BUILD, "api_fp64.cu.o")
+    _compile(os.path.join(CSRC, "api.cu"), api_fp64, deps, verbose, defines=("MF_CG_INC_FP64",))
+    _link(OUT, objs)
+    _link(OUT_FP64, [api_fp64 if o.endswith("api.cu.o") else o for o in objs])
     build_drivers(verbose)
     return OUT
 
@@ -76,10 +90,12 @@ def build_drivers(verbose: bool = False) -> None:
     src = os.path.join(CSRC, "driver_main.cpp")
     for k, name in enumerate(DRIVERS):
         exe = os.path.join(BIN, name)
-        if not _newer(src, exe, [OUT, os.path.join(INCLUDE, "millefeuille.h")]):
+        # main-cg replaces main-cg.cu, whose cg_solve_inc is FP64
+        lib = OUT_FP64 if name == "main-cg" else OUT
+        if not _newer(src, exe, [lib, os.path.join(INCLUDE, "millefeuille.h")]):
             continue
         cmd = ["g++", "-O2", "-std=c++17", f"-DMF_DRIVER={k}", "-I", INCLUDE, src, "-o", exe,
-               "-L", os.path.dirname(OUT), "-lmillefeuille", "-Wl,-rpath,$ORIGIN/../millefeuille"]
+               "-L", os.path.dirname(OUT), "-l" + os.path.basename(lib)[3:-3], "-Wl,-rpath,$ORIGIN/../millefeuille"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if verbose or r.returncode:
             sys.stderr.write(r.stdout + r.stderr)

@@ -43,7 +43,11 @@ const char *mf_status_string(int status)
     }
 }
 
+#ifdef MF_CG_INC_FP64
+const char *mf_build_arch(void) { return "sm_100a (cg_solve_inc: FP64, main-cg.cu)"; }
+#else
 const char *mf_build_arch(void) { return "sm_100a"; }
+#endif
 
 void mf_options_default(mf_options *o)
 {
@@ -525,6 +529,9 @@ void append_csv(const char *csv, const char *filename, const char *line)
     fclose(f);
 }
 
+// The full report of the calling thread's last drop-in solve (mf_dropin_last_report).
+thread_local mf_report g_dropin_report;
+
 // Shared body of the cg_solve_* shims (main-cg-mixed.cu:2248-3069 / main-cg.cu).
 void cg_dropin(int precision, const char *csv, int *RowPtr, int *ColIdx, double *Val, float *Val_Low, double *x,
                double *b, int n, char *filename, int nnzR, int ori, int max_iter, CgBenchResult *bench_result,
@@ -543,7 +550,9 @@ void cg_dropin(int precision, const char *csv, int *RowPtr, int *ColIdx, double 
         o.fixed_iters = 1;
         o.replace_every = 0;
         mf_report rep;
+        memset(&rep, 0, sizeof(rep));
         rc = mf_solve(A, b, x, &o, &rep, 0, nullptr);
+        g_dropin_report = rep;
         res.time_ms = rep.time_ms;
         res.iterations = rep.iterations;
         res.l2_norm = rep.relres_true;
@@ -588,6 +597,7 @@ int bicg_dropin(int precision, const char *csv, int *RowPtr, int *ColIdx, double
         rc = mf_solve(A, rhs, x, &o, &rep, 0, nullptr);
         mf_matrix_destroy(A);
     }
+    g_dropin_report = rep;
     if (rc != MF_SUCCESS) fprintf(stderr, "millefeuille: %s\n", mf_status_string(rc));
     printf("time_bicg=%lf ms\n", rep.time_ms);
     char line[256];
@@ -599,13 +609,31 @@ int bicg_dropin(int precision, const char *csv, int *RowPtr, int *ColIdx, double
 
 }  // namespace
 
+// The reference has two cg_solve_inc with one signature: the mixed-precision
+// solver of main-cg-mixed.cu:2248 and the FP64 one of main-cg.cu:1110 (which
+// main-cg calls for nnz < 10,000, main-cg.cu:1727-1745).  libmillefeuille.so
+// exports the mixed one; libmillefeuille_fp64.so, the same objects with this
+// file compiled with MF_CG_INC_FP64, exports the FP64 one, for programs that
+// link main-cg.cu's entry points.
 extern "C" void cg_solve_inc(int *RowPtr, int *ColIdx, double *Val, float *Val_Low, double *x, double *b, int n,
                              int *iter, int maxiter, double threshold, char *filename, int nnzR, int ori,
                              int max_iter, CgBenchResult *bench_result, int skip_output)
 {
     (void)iter; (void)maxiter; (void)threshold;
+#ifdef MF_CG_INC_FP64
+    cg_dropin(MF_PREC_FP64, "cg_performance.csv", RowPtr, ColIdx, Val, Val_Low, x, b, n, filename, nnzR, ori,
+              max_iter, bench_result, skip_output);
+#else
     cg_dropin(MF_PREC_MIXED, "cg_mixed_performance.csv", RowPtr, ColIdx, Val, Val_Low, x, b, n, filename, nnzR,
               ori, max_iter, bench_result, skip_output);
+#endif
+}
+
+extern "C" int mf_dropin_last_report(mf_report *out)
+{
+    if (!out) return MF_ERR_INVALID;
+    *out = g_dropin_report;
+    return MF_SUCCESS;
 }
 
 extern "C" void cg_solve_sync(int *RowPtr, int *ColIdx, double *Val, float *Val_Low, double *x, double *b, int n,

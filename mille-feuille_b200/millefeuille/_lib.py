@@ -10,6 +10,8 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libmillefeuille.so")
+# the same library with cg_solve_inc in FP64 (main-cg.cu's entry point)
+LIB_FP64_PATH = os.path.join(HERE, "libmillefeuille_fp64.so")
 
 MF_SUCCESS, MF_ERR_INVALID, MF_ERR_CUDA, MF_ERR_NOMEM, MF_ERR_TIMEOUT = 0, 1, 2, 3, 4
 MF_ERR_UNSUPPORTED, MF_ERR_BREAKDOWN, MF_ERR_IO, MF_ERR_NOT_BUILT = 5, 6, 7, 8
@@ -70,6 +72,7 @@ EXPORTED = [
     "mf_debug_ref_labels", "mf_build_arch", "mf_spmv_noalloc", "mf_value_grad", "mf_matrix_create_transposed",
     "mf_solve_multi", "mf_batch_create", "mf_batch_tune", "mf_batch_solve", "mf_batch_destroy",
     "mf_batch_partition", "mf_batch_schedule", "mf_debug_spmv_tiles", "mf_debug_solver_labels",
+    "mf_dropin_last_report",
 ]
 
 _lib = None
@@ -108,6 +111,7 @@ def load() -> C.CDLL:
     L.mf_debug_ref_labels.argtypes = [vp, vp, C.c_int, vp, C.c_int]
     L.mf_debug_spmv_tiles.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.mf_debug_solver_labels.argtypes = [vp, vp, C.c_int]
+    L.mf_dropin_last_report.argtypes = [C.POINTER(Report)]
     L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
     L.mf_write_cbd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp]
     L.mf_free_host.argtypes = [vp]
