@@ -141,6 +141,14 @@ typedef struct {
                               of its maximum in the previous update (or of the tiles are exact in a
                               narrower type, for use_lossless); below it every tile runs FP32.
                               Default 0.125; 0 = always consider them */
+    double relax_eta;      /* mixed CG (mf_solve): relaxed matvec precision.  Once the recursive
+                              relative residual rho has fallen so far that relax_eta * tol / rho
+                              exceeds a stored precision's rounding (2^-11 FP16, 2^-8 scaled
+                              INT8, see relax_int8), the whole SpMV runs in it (inexact Krylov
+                              relaxation; the FP64 residual replacement and the FP64 convergence
+                              test keep the final accuracy).  0 = off */
+    int relax_int8;        /* with relax_eta: the relaxed precision may go down to scaled INT8
+                              (default 0: FP16 at most) */
 } mf_options;
 
 typedef struct {

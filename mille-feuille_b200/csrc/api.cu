@@ -68,6 +68,8 @@ void mf_options_default(mf_options *o)
     o->l2_window = 1;
     o->test_stall_barrier = 0;
     o->demote_min_fraction = 0.125;
+    o->relax_eta = 0.0;
+    o->relax_int8 = 0;
 }
 
 void mf_free_host(void *p) { free(p); }

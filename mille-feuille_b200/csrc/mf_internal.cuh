@@ -99,6 +99,7 @@ struct mf_matrix_s {
     // tiles exact in INT8 or FP16 (counted on first use; n_exact_known = 0 before)
     int n_exact_known;
     long long n_exact;
+    long long n_fp16_ok;       // tiles whose values lie within FP16's normal range
 };
 
 // Position of entry k of row i in the slice whose payload starts at entry

@@ -74,6 +74,9 @@ struct SolverParams {
     float demote16, demote8;
     unsigned long long timeout_ns;
     int stall_first_barrier;   // test hook: first barrier expects one extra arrival
+    float relax_eta;           // mixed CG: relaxation factor of the matvec precision (0: off)
+    int relax_int8;            // the relaxation may go down to scaled INT8 (else FP16 at most)
+    int fp16_ok;               // every tile's values are within FP16's normal range
 };
 
 struct Shared {
@@ -436,40 +439,84 @@ __device__ __forceinline__ double slice_dot_parity(const SolverParams &P, int4 h
 // Mixed mode when no tile can leave FP32 in this SpMV: every slice runs the
 // FP32 chunk loop directly (no per-slice precision reduction); the range's tile
 // and entry totals go to the counters once, at the end.
+// Lane i's FP32 values and index word of the chunk at entry offset cb
+// (unpredicated: the stored padding past a row's end is zero).
+__device__ __forceinline__ void load_chunk_f32(const SolverParams &P, long long cb, int i, float4 &a, float4 &b,
+                                               unsigned long long &m)
+{
+    a = __ldcs((const float4 *)(P.v32 + cb) + i);
+    b = __ldcs((const float4 *)(P.v32 + cb + 64) + i);
+    m = __ldcs((const unsigned long long *)(P.meta + cb) + i);
+}
+
+// Mixed mode when no tile can leave FP32 in this SpMV: every slice runs FP32
+// stored values (no per-slice precision reduction); the range's tile and
+// entry totals go to the counters once, at the end.
+// The walk is software-pipelined by one chunk.  A half-warp's slices are
+// stored back to back, so its chunks (kp / 8 per slice) form one contiguous
+// stream and chunk c + 1 starts 128 entries after chunk c whatever slice it
+// belongs to: its values and index word are requested as soon as chunk c's x
+// gathers are issued, so their DRAM trip overlaps chunk c's gathers, sum and
+// tile-row epilogue instead of following them.  Sums are formed in the same
+// order as slice_dot_uniform (per slice from 0, added to the tile-row's sum).
 template <typename Epi>
 __device__ __forceinline__ void spmv_range_f32(const SolverParams &P, int sb, int se, int i, unsigned hmask,
                                                const XVec &X, unsigned *cnt, Epi &epi)
 {
     int4 h = P.seg_hdr[sb];
+    const int4 hl = P.seg_hdr[se - 1];
+    const long long off0 = hdr_off(h);
+    const int nch = (int)((hdr_off(hl) + (long long)hdr_kp(hl) * MF_BS - off0) >> 7);
     int tw = P.seg_tile[(long long)sb * MF_BS + i];
     int len = P.seg_rowlen[(long long)sb * MF_BS + i];
-    long long off = hdr_off(h);
-    double acc = 0.0;
+    float4 a, b;
+    unsigned long long m8;
+    load_chunk_f32(P, off0, i, a, b, m8);
+    int4 hn = make_int4(0, 0, 0, 0);
+    int twn = 0, lenn = 0;
+    int s = sb, kc = 0, kchunks = hdr_kp(h) >> 3;
     unsigned ntiles = 0, nent = 0;
-    auto nopre = [&]() {};
-    for (int s = sb; s < se; s++) {
-        const bool more = s + 1 < se;
-        int4 hn = make_int4(0, 0, 0, 0);
-        int twn = 0, lenn = 0;
-        if (more) {
+    double acc = 0.0, sacc = 0.0;
+    for (int c = 0; c < nch; c++) {
+        if (kc == 0 && s + 1 < se) {       // the next slice's words, one slice ahead
             hn = P.seg_hdr[s + 1];
             twn = P.seg_tile[(long long)(s + 1) * MF_BS + i];
             lenn = P.seg_rowlen[(long long)(s + 1) * MF_BS + i];
         }
-        TileReg T;
-        T.xb = (tw >> 8) * MF_BS;
-        T.pr = MF_P32;
-        ntiles += (unsigned)hdr_nt(h);
-        nent += (unsigned)len;
-        acc += slice_dot_uniform<MF_P32>(P, h, off, i, hmask, len, T, X, nopre);
-        if (hdr_last(h)) {
-            epi(h.y, acc);
-            acc = 0.0;
+        const int k0 = kc * 8;
+        const int xb = (tw >> 8) * MF_BS;
+        double xv[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+            const int xi = __shfl_sync(hmask, xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
+            xv[j] = (k0 + j < len) ? X.x64[xi] : 0.0;
         }
-        off += (long long)hdr_kp(h) * MF_BS;
-        h = hn;
-        tw = twn;
-        len = lenn;
+        float4 an = make_float4(0.f, 0.f, 0.f, 0.f), bn = an;
+        unsigned long long mn = 0ull;
+        if (c + 1 < nch) load_chunk_f32(P, off0 + (long long)(c + 1) * 128, i, an, bn, mn);
+        const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int j = 0; j < 8; j++) sacc = fma((double)v[j], xv[j], sacc);
+        if (++kc == kchunks) {             // the slice is done
+            ntiles += (unsigned)hdr_nt(h);
+            nent += (unsigned)len;
+            acc += sacc;
+            sacc = 0.0;
+            if (hdr_last(h)) {
+                epi(h.y, acc);
+                acc = 0.0;
+            }
+            s++;
+            h = hn;
+            tw = twn;
+            len = lenn;
+            kc = 0;
+            kchunks = hdr_kp(h) >> 3;
+        }
+        a = an;
+        b = bn;
+        m8 = mn;
     }
     if (cnt) {
         nent = __reduce_add_sync(hmask, nent);
@@ -697,6 +744,27 @@ __device__ __forceinline__ bool restart_after_replacement(bool failed_check, dou
     return failed_check || rr_true > 4.0 * rr_rec || 4.0 * rr_true < rr_rec;
 }
 
+// Relaxed matvec precision (mixed CG): inexact Krylov theory (van den Eshof &
+// Sleijpen, SIAM J. Matrix Anal. Appl. 26(1), 2004; Bouras & Fraysse, SIAM J.
+// Matrix Anal. Appl. 26(3), 2005) lets the relative error of the product at
+// iteration k grow like eps_k = eta * tol / (||r_k|| / ||b||): the further the
+// solve has converged, the coarser the operator may be.  The whole SpMV then
+// runs in the narrowest stored precision whose rounding stays below eps_k:
+// FP16 (unit roundoff 2^-11) when every tile fits FP16's normal range and,
+// when allowed, scaled INT8 (half a step of the tile's largest magnitude /
+// 127, below 2^-8 of it).  The FP64 residual replacement and the convergence
+// test on the FP64 true residual keep the final accuracy either way.
+constexpr double kRoundF16 = 1.0 / 2048.0;
+constexpr double kRoundI8 = 1.0 / 256.0;
+__device__ __forceinline__ int relaxed_precision(const SolverParams &P, double rr, double bb)
+{
+    if (P.relax_eta <= 0.0f || !(bb > 0.0) || !(rr > 0.0)) return MF_P32;
+    const double eps = (double)P.relax_eta * P.tol / sqrt(rr / bb);
+    if (P.relax_int8 && eps >= kRoundI8) return MF_P8;
+    if (eps >= kRoundF16 && P.fp16_ok) return MF_P16;
+    return MF_P32;
+}
+
 template <int MODE, int LB>
 __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
 {
@@ -798,6 +866,8 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     bool has_empty = false;
     for (int R = c.rbeg; R < c.rend && !has_empty; R++) has_empty = P.seg_ptr[R] == P.seg_ptr[R + 1];
     double beta2 = 0.0;
+    // mixed CG: uniform reduced precision of the next SpMV (relaxed_precision)
+    int prA = (MODE == MODE_MIXED) ? relaxed_precision(P, rr, bb) : MF_P32;
 
     while (!conv && k < P.max_iter) {
         if (MODE != MODE_PARITY && !bicg) {
@@ -807,19 +877,20 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             // are the textbook CG scalars (main-cg-mixed.cu:1224-1382 keeps the
             // same formulas with the SpMV on p and a third sync).
             // ---- A: w = A r; p = r + beta p; q = w + beta q; p.q ----
+            // (mixed: with a relaxed precision prA the whole SpMV runs in it)
             double ppq = 0.0;
-            spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
-                                    make_x(P.r, nullptr, nullptr, nullptr, P.mag_r, nullptr, invM, dynA), cnt,
-                                    [&](int R, double y) {
-                                        const int row = R * MF_BS + c.i;
-                                        if (row < n) {
-                                            const double pn = P.r[row] + beta2 * P.p[row];
-                                            const double qn = y + beta2 * P.q[row];
-                                            P.p[row] = pn;
-                                            P.q[row] = qn;
-                                            ppq += pn * qn;
-                                        }
-                                    });
+            XVec XA = make_x(P.r, nullptr, nullptr, nullptr, P.mag_r, nullptr, invM, dynA);
+            if (MODE == MODE_MIXED && prA != MF_P32) XA.force_pr = prA;
+            spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask, XA, cnt, [&](int R, double y) {
+                const int row = R * MF_BS + c.i;
+                if (row < n) {
+                    const double pn = P.r[row] + beta2 * P.p[row];
+                    const double qn = y + beta2 * P.q[row];
+                    P.p[row] = pn;
+                    P.q[row] = qn;
+                    ppq += pn * qn;
+                }
+            });
             if (has_empty) {
                 for (int R = c.rbeg; R < c.rend; R++) {
                     if (P.seg_ptr[R] != P.seg_ptr[R + 1]) continue;
@@ -937,6 +1008,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             }
             beta2 = restart ? 0.0 : rr_new / rr;
             rr = rr_new;
+            if (MODE == MODE_MIXED) prA = relaxed_precision(P, rr, bb);
             continue;
         }
         double alpha = 0.0, omega = 0.0;
@@ -2163,27 +2235,34 @@ int dal(T **p, long long count)
         if (_rc != MF_SUCCESS) return _rc;  \
     } while (0)
 
+// count[0]: tiles exact in INT8 or FP16; count[1]: tiles within FP16's normal range
 __global__ void k_count_exact(const unsigned char *caps, int n, unsigned long long *count)
 {
-    unsigned c = 0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    unsigned c = 0, h = 0;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         if (caps[t] & (MF_CAP_EXACT_I8 | MF_CAP_EXACT_F16)) c++;
+        if (caps[t] & MF_CAP_FP16_OK) h++;
+    }
     c = __reduce_add_sync(0xffffffffu, c);
+    h = __reduce_add_sync(0xffffffffu, h);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+    if ((threadIdx.x & 31) == 0 && h) atomicAdd(count + 1, (unsigned long long)h);
 }
 
-// Tiles exact in INT8 or FP16 (the lossless classes), counted once per matrix
-// through `scratch` (one unsigned long long of device memory).
+// Tiles exact in INT8 or FP16 (the lossless classes) and tiles within FP16's
+// normal range, counted once per matrix through `scratch` (two unsigned long
+// long of device memory).
 int exact_tiles(mf_matrix_s *A, unsigned long long *scratch, cudaStream_t s)
 {
     if (!A->n_exact_known) {
-        unsigned long long h = 0;
+        unsigned long long h[2] = {0, 0};
         MF_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(h), s));
         if (A->tilenum > 0) k_count_exact<<<256, 256, 0, s>>>(A->d_tile_caps, A->tilenum, scratch);
         MF_CUDA_TRY(cudaGetLastError());
-        MF_CUDA_TRY(cudaMemcpyAsync(&h, scratch, sizeof(h), cudaMemcpyDeviceToHost, s));
+        MF_CUDA_TRY(cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, s));
         MF_CUDA_TRY(cudaStreamSynchronize(s));
-        A->n_exact = (long long)h;
+        A->n_exact = (long long)h[0];
+        A->n_fp16_ok = (long long)h[1];
         A->n_exact_known = 1;
     }
     return MF_SUCCESS;
@@ -2428,6 +2507,9 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     P.use_lossless = opt->use_lossless;
     P.lossless_any = lossless_on(opt->use_lossless, opt->demote_min_fraction, A->n_exact, A->tilenum);
     P.min_small = (float)(opt->demote_min_fraction * (double)A->tilem);
+    P.relax_eta = (float)opt->relax_eta;
+    P.relax_int8 = opt->relax_int8 ? 1 : 0;
+    P.fp16_ok = A->n_fp16_ok == A->tilenum ? 1 : 0;
     P.tol = opt->tol;
     P.demote16 = (float)opt->demote_fp16;
     P.demote8 = (float)opt->demote_int8;
@@ -2898,7 +2980,7 @@ int batch_build_items(BatchImpl &B, int cap, int lb, cudaStream_t s)
     {
         // exact-tile counts of the systems (once per matrix)
         unsigned long long *scratch = nullptr;
-        MF_CUDA_TRY(cudaMalloc((void **)&scratch, sizeof(*scratch)));
+        MF_CUDA_TRY(cudaMalloc((void **)&scratch, 2 * sizeof(*scratch)));
         int rc = MF_SUCCESS;
         for (mf_matrix_s *A : B.sys)
             if (rc == MF_SUCCESS) rc = exact_tiles(A, scratch, s);

@@ -30,7 +30,8 @@ class Options(C.Structure):
                 ("fixed_iters", C.c_int), ("replace_every", C.c_int), ("demote_fp16", C.c_double),
                 ("demote_int8", C.c_double), ("use_lossless", C.c_int), ("wait_timeout_s", C.c_double),
                 ("blocks_per_sm", C.c_int), ("threads_per_block", C.c_int), ("x0_given", C.c_int),
-                ("l2_window", C.c_int), ("test_stall_barrier", C.c_int), ("demote_min_fraction", C.c_double)]
+                ("l2_window", C.c_int), ("test_stall_barrier", C.c_int), ("demote_min_fraction", C.c_double),
+                ("relax_eta", C.c_double), ("relax_int8", C.c_int)]
 
 
 class Report(C.Structure):

@@ -269,3 +269,18 @@ def test_gpu_initial_guess(mf, cuda, p3d, cd3d, method, precision):
     xd, rd = G.solve(bd, xd, method=method, precision=precision, tol=1e-10, x0_given=1)
     assert rd["iterations"] == rw["iterations"]
     np.testing.assert_array_equal(xd.cpu().numpy(), xw)
+
+
+def test_gpu_relaxed_precision_converges_and_uses_fp16(mf, cuda, p3d):
+    """relax_eta: once relax_eta * tol / (||r|| / ||b||) exceeds FP16's unit
+    roundoff, the whole SpMV runs on FP16 stored values.  The solve still
+    converges on its FP64 true residual (host-checked), FP16 tiles were used,
+    and relax_eta = 0 uses none (this system has no exact-FP16 tiles)."""
+    A, b, _ = p3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x0, r0 = G.solve(b, method="cg", precision="mixed", tol=1e-8)
+    assert r0["tile_uses"][2] == 0 and r0["tile_uses"][3] == 0, r0["tile_uses"]
+    x, rep = G.solve(b, method="cg", precision="mixed", tol=1e-8, relax_eta=1.0)
+    assert rep["converged"] and rep["relres_true"] <= 1e-8
+    assert _relres(A, x, b) <= 1.0001e-8
+    assert rep["tile_uses"][2] > 0 and rep["tile_uses"][3] == 0, rep["tile_uses"]
