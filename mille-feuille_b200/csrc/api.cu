@@ -11,7 +11,18 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 static thread_local char g_last_err[512];
+
+namespace {
+// NVTX range around a C-ABI call, so profilers (ncu --nvtx, Nsight Systems)
+// can attribute kernels to the call that launched them; free without a tool.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+}  // namespace
 
 void mf_set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line)
 {
@@ -136,6 +147,7 @@ extern "C" int mf_matrix_create(mf_matrix *out, int n_rows, int n_cols, long lon
                                 const int *colidx, const double *val, const float *val_low, int device_ptrs,
                                 void *stream)
 {
+    NvtxRange nvtx_range("mf_matrix_create");
     if (!out || n_rows < 0 || n_cols < 0 || nnz < 0 || !rowptr || (nnz > 0 && (!colidx || !val)))
         return MF_ERR_INVALID;
     if (nnz >= (1LL << 31)) return MF_ERR_UNSUPPORTED;
@@ -305,6 +317,7 @@ extern "C" int mf_tile_export(mf_matrix A, const char *name, void *host_dst, siz
 extern "C" int mf_solve(mf_matrix A, const double *b, double *x, const mf_options *opt, mf_report *report,
                         int device_ptrs, void *stream)
 {
+    NvtxRange nvtx_range("mf_solve");
     if (!A || !b || !x) return MF_ERR_INVALID;
     mf_options o;
     if (opt) o = *opt; else mf_options_default(&o);
@@ -341,6 +354,7 @@ extern "C" int mf_solve(mf_matrix A, const double *b, double *x, const mf_option
 extern "C" int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_options *opt,
                               mf_report *reports, int device_ptrs, void *stream)
 {
+    NvtxRange nvtx_range("mf_solve_multi");
     if (!A || !B || !X || nrhs < 1) return MF_ERR_INVALID;
     if (A->n_rows != A->n_cols) return MF_ERR_INVALID;
     mf_options o;
@@ -386,6 +400,7 @@ extern "C" int mf_batch_tune(mf_batch b, int precision, int iters, int *chosen_c
 extern "C" int mf_batch_solve(mf_batch b, const double *const *B, double *const *X, const mf_options *opt,
                               mf_report *reports, int use_graph, void *stream)
 {
+    NvtxRange nvtx_range("mf_batch_solve");
     if (!b || !B || !X) return MF_ERR_INVALID;
     mf_options o;
     if (opt) o = *opt;
@@ -447,6 +462,7 @@ extern "C" int mf_batch_partition(int nsys, const int *n, const long long *nnz, 
 extern "C" int mf_spmv(mf_matrix A, const double *x, double *y, int precision, int device_ptrs, void *stream,
                        double *elapsed_ms)
 {
+    NvtxRange nvtx_range("mf_spmv");
     if (!A || !x || !y) return MF_ERR_INVALID;
     if (precision != MF_PREC_FP64 && precision != MF_PREC_MIXED) return MF_ERR_INVALID;
     cudaStream_t s = (cudaStream_t)stream;

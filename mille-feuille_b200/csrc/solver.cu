@@ -2218,8 +2218,11 @@ struct Workspace {
     int m_nr, m_G;
     double *m_vec;         // B | X | R | P | Q, each vec_len * NR
     float *m_mag;
-    double *m_red, *m_out;
+    double *m_red, *m_out; // m_out: one result record per column group of a call (m_groups of them)
+    int *m_err;            // one error word per column group
     int *m_hw_begin;
+    int m_groups;          // column-group slots of m_out / m_err / m_ev
+    cudaEvent_t *m_ev;     // two timing events per column group
 };
 
 template <typename T>
@@ -2451,9 +2454,11 @@ void mf_solver_free_ws(mf_matrix_s *A)
     Workspace *w = (Workspace *)A->ws;
     if (!w) return;
     void *ptrs[] = {w->vecs, w->mag_p, w->mag_s, w->lab_p, w->lab_s, w->red, w->bar, w->err, w->out, w->counts,
-                    w->phase_ns, w->hw_begin, w->m_vec, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
+                    w->phase_ns, w->hw_begin, w->m_vec, w->m_mag, w->m_red, w->m_out, w->m_err, w->m_hw_begin};
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    for (int k = 0; k < 2 * w->m_groups; k++) cudaEventDestroy(w->m_ev[k]);
+    delete[] w->m_ev;
     cudaEventDestroy(w->e0);
     cudaEventDestroy(w->e1);
     delete w;
@@ -2740,10 +2745,10 @@ const void *multi_kernel(int mode, int nr)
 int ws_multi(mf_matrix_s *A, Workspace *w, int mode, int nr, cudaStream_t s)
 {
     if (w->m_nr == nr && w->m_vec) return MF_SUCCESS;
-    void *old[] = {w->m_vec, w->m_mag, w->m_red, w->m_out, w->m_hw_begin};
+    void *old[] = {w->m_vec, w->m_mag, w->m_red, w->m_hw_begin};
     for (void *p : old)
         if (p) cudaFree(p);
-    w->m_vec = nullptr; w->m_mag = nullptr; w->m_red = nullptr; w->m_out = nullptr;
+    w->m_vec = nullptr; w->m_mag = nullptr; w->m_red = nullptr;
     w->m_hw_begin = nullptr;
     w->m_nr = 0;
     int dev = 0, nsm = 0, occ = 0;
@@ -2762,7 +2767,6 @@ int ws_multi(mf_matrix_s *A, Workspace *w, int mode, int nr, cudaStream_t s)
     MF_TRY(dal(&w->m_vec, 5 * L * nr));
     MF_TRY(dal(&w->m_mag, S));
     MF_TRY(dal(&w->m_red, (long long)kRedKinds * G * kRedWidthM));
-    MF_TRY(dal(&w->m_out, 4 * kMaxNR + 8));
     MF_TRY(dal(&w->m_hw_begin, (long long)G * kWarps * 2 + 1));
     MF_CUDA_TRY(cudaMemsetAsync(w->m_vec, 0, (size_t)5 * L * nr * sizeof(double), s));
     MF_CUDA_TRY(cudaMemsetAsync(w->m_mag, 0, (size_t)S * sizeof(float), s));
@@ -2771,6 +2775,28 @@ int ws_multi(mf_matrix_s *A, Workspace *w, int mode, int nr, cudaStream_t s)
     MF_CUDA_TRY(cudaGetLastError());
     w->m_G = G;
     w->m_nr = nr;
+    return MF_SUCCESS;
+}
+
+constexpr int kOutM = 4 * kMaxNR + 8;    // doubles per column group's result record
+
+// Result slots for `groups` column groups (grown, never shrunk).
+int ws_multi_groups(Workspace *w, int groups)
+{
+    if (w->m_groups >= groups) return MF_SUCCESS;
+    if (w->m_out) cudaFree(w->m_out);
+    if (w->m_err) cudaFree(w->m_err);
+    w->m_out = nullptr;
+    w->m_err = nullptr;
+    for (int k = 0; k < 2 * w->m_groups; k++) cudaEventDestroy(w->m_ev[k]);
+    delete[] w->m_ev;
+    w->m_ev = nullptr;
+    w->m_groups = 0;
+    MF_TRY(dal(&w->m_out, (long long)groups * kOutM));
+    MF_TRY(dal(&w->m_err, groups));
+    w->m_ev = new cudaEvent_t[2 * groups];
+    for (int k = 0; k < 2 * groups; k++) MF_CUDA_TRY(cudaEventCreate(&w->m_ev[k]));
+    w->m_groups = groups;
     return MF_SUCCESS;
 }
 
@@ -2812,43 +2838,50 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
     M.Q = w->m_vec + 4 * L * nr;
     M.mag = w->m_mag;
     M.red = w->m_red;
-    M.out = w->m_out;
     const int groups = (nrhs + nr - 1) / nr;
-    int first_err = MF_SUCCESS;
+    MF_TRY(ws_multi_groups(w, groups));
+    MF_CUDA_TRY(cudaMemsetAsync(w->m_out, 0, (size_t)groups * kOutM * sizeof(double), s));
+    MF_CUDA_TRY(cudaMemsetAsync(w->m_err, 0, (size_t)groups * sizeof(int), s));
+    // every column group is enqueued back to back (the interleaved buffers are
+    // reused in stream order); the host reads the results once, at the end
     for (int g = 0; g < groups; g++) {
         M.nr = std::min(nr, nrhs - g * nr);
+        M.out = w->m_out + (size_t)g * kOutM;
+        P.err = w->m_err + g;
         k_interleave<<<592, 256, 0, s>>>(d_B, n, (int)L, nrhs, g, nr, (double *)M.B);
         if (opt->x0_given) k_interleave<<<592, 256, 0, s>>>(d_X, n, (int)L, nrhs, g, nr, M.X);
         MF_CUDA_TRY(cudaGetLastError());
         MF_CUDA_TRY(cudaMemsetAsync(w->bar, 0, sizeof(unsigned int), s));
-        MF_CUDA_TRY(cudaMemsetAsync(w->err, 0, sizeof(int), s));
-        MF_CUDA_TRY(cudaMemsetAsync(w->m_out, 0, (4 * kMaxNR + 8) * sizeof(double), s));
         void *args[] = {&P, &M};
-        MF_CUDA_TRY(cudaEventRecord(w->e0, s));
+        MF_CUDA_TRY(cudaEventRecord(w->m_ev[2 * g], s));
         MF_CUDA_TRY(cudaLaunchCooperativeKernel(multi_kernel(mode, nr), dim3(w->m_G), dim3(kThreads), args, 0, s));
-        MF_CUDA_TRY(cudaEventRecord(w->e1, s));
+        MF_CUDA_TRY(cudaEventRecord(w->m_ev[2 * g + 1], s));
         k_deinterleave<<<592, 256, 0, s>>>(M.X, n, nrhs, g, nr, d_X);
         MF_CUDA_TRY(cudaGetLastError());
-        double out[4 * kMaxNR + 8];
-        int err = 0;
-        MF_CUDA_TRY(cudaMemcpyAsync(out, w->m_out, sizeof(out), cudaMemcpyDeviceToHost, s));
-        MF_CUDA_TRY(cudaMemcpyAsync(&err, w->err, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MF_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    std::vector<double> out((size_t)groups * kOutM);
+    std::vector<int> err(groups);
+    MF_CUDA_TRY(cudaMemcpyAsync(out.data(), w->m_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MF_CUDA_TRY(cudaMemcpyAsync(err.data(), w->m_err, err.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    MF_CUDA_TRY(cudaStreamSynchronize(s));
+    int first_err = MF_SUCCESS;
+    for (int g = 0; g < groups; g++) {
+        const double *o = out.data() + (size_t)g * kOutM;
         float ms = 0.f;
-        MF_CUDA_TRY(cudaEventElapsedTime(&ms, w->e0, w->e1));
-        const int status = err ? err : (int)out[4 * nr + 1];
+        MF_CUDA_TRY(cudaEventElapsedTime(&ms, w->m_ev[2 * g], w->m_ev[2 * g + 1]));
+        const int status = err[g] ? err[g] : (int)o[4 * nr + 1];
         if (status != MF_SUCCESS && first_err == MF_SUCCESS) first_err = status;
         if (reps) {
-            for (int k = 0; k < M.nr; k++) {
+            for (int k = 0; k < std::min(nr, nrhs - g * nr); k++) {
                 mf_report *r = &reps[g * nr + k];
                 memset(r, 0, sizeof(*r));
                 r->status = status;
-                r->iterations = (int)out[4 * k + 0];
-                r->converged = (int)out[4 * k + 1];
-                r->relres_true = out[4 * k + 2];
-                r->relres_rec = out[4 * k + 3];
+                r->iterations = (int)o[4 * k + 0];
+                r->converged = (int)o[4 * k + 1];
+                r->relres_true = o[4 * k + 2];
+                r->relres_rec = o[4 * k + 3];
                 r->time_ms = ms;
-                r->replacements = (int)out[4 * nr + 2];
+                r->replacements = (int)o[4 * nr + 2];
                 r->grid_blocks = w->m_G;
                 r->threads_per_block = kThreads;
             }

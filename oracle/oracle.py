@@ -50,9 +50,13 @@ class OrcReport(C.Structure):
                 ("relres_true", C.c_double), ("replacements", C.c_int)]
 
 
-def build() -> None:
-    """Compile the oracle (and the reference harness when the tree exists)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+def build(ref_src: str | None = None) -> None:
+    """Compile the oracle, and the reference-host harness when ref_src (the
+    reference tree's src/ directory) is given."""
+    cmd = ["make", "-s", "-C", HERE]
+    if ref_src:
+        cmd.append(f"REF_SRC={ref_src}")
+    subprocess.run(cmd, check=True)
 
 
 def _load():

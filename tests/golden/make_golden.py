@@ -57,7 +57,7 @@ def sha(a: np.ndarray) -> str:
 
 def main():
     if not oracle.ref_available():
-        raise SystemExit("oracle/_ref/libmf_refhost.so is missing: run `make -C oracle` with the reference tree")
+        raise SystemExit("oracle/_ref/libmf_refhost.so is missing: run `make -C oracle REF_SRC=<reference>/src`")
     out = {}
     for name, rowA, colA, A in small_cases():
         dims, arrs = oracle.ref_tile_create(rowA, colA, A.rowptr, A.colidx, A.val)
