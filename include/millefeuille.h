@@ -368,6 +368,17 @@ int mf_debug_ref_labels(const double *p_old, const double *p_new, int nseg, int 
  * the solver, in half / int8 arithmetic). */
 int mf_debug_spmv_tiles(mf_matrix A, const double *x, double *y, int tile_prec, int device_ptrs);
 
+/* Experiment hook: Y = A X for 8 right-hand sides (columns one after another,
+ * n_cols / n_rows doubles each) with every tile's values stored in FP16.
+ * tensor_cores = 0: the solver's CUDA-core arithmetic (FP16 value widened to
+ * FP64 against the FP64 X); 1: each 16 x 16 tile densified in shared memory
+ * from the sparse payload and multiplied with the FP16-rounded 16 x 8 block
+ * of X by one mma.sync.m16n8k16 per tile (FP32 accumulation).  elapsed_ms
+ * (nullable): the kernel's time.  Host pointers unless device_ptrs != 0.
+ * No counterpart in the reference. */
+int mf_debug_spmm(mf_matrix A, const double *X, double *Y, int tensor_cores, int device_ptrs,
+                  double *elapsed_ms);
+
 /* Test hook: the labels the last mf_solve on A in MF_PREC_PARITY left for the
  * next SpMV's operand p (d_vis codes: 0 FP64, 4 FP32, 3 FP16, 2 INT8, 1
  * bypass), one per column segment (main-cg-mixed.cu:1323-1370 computes them);

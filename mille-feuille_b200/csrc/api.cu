@@ -503,6 +503,24 @@ extern "C" int mf_debug_spmv_tiles(mf_matrix A, const double *x, double *y, int 
     return rc;
 }
 
+extern "C" int mf_debug_spmm(mf_matrix A, const double *X, double *Y, int tensor_cores, int device_ptrs,
+                             double *elapsed_ms)
+{
+    if (!A || !X || !Y) return MF_ERR_INVALID;
+    const size_t nx = (size_t)8 * A->n_cols, ny = (size_t)8 * A->n_rows;
+    const double *dX = X;
+    double *dY = Y, *tmp = nullptr;
+    if (!device_ptrs) {
+        MF_TRY(stage_get(A, (nx + ny) * sizeof(double), &tmp));
+        MF_CUDA_TRY(cudaMemcpy(tmp, X, nx * sizeof(double), cudaMemcpyHostToDevice));
+        dX = tmp;
+        dY = tmp + nx;
+    }
+    int rc = mf_spmm_run(A, dX, dY, tensor_cores ? 1 : 0, 0, elapsed_ms);
+    if (!device_ptrs && rc == MF_SUCCESS) MF_CUDA_TRY(cudaMemcpy(Y, dY, ny * sizeof(double), cudaMemcpyDeviceToHost));
+    return rc;
+}
+
 extern "C" int mf_debug_solver_labels(mf_matrix A, int *vis, int nseg)
 {
     if (!A || (nseg > 0 && !vis)) return MF_ERR_INVALID;

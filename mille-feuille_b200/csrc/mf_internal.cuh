@@ -167,6 +167,8 @@ int mf_spmv_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, c
 int mf_spmv_tiles_run(mf_matrix_s *A, const double *d_x, double *d_y, int tile_prec, cudaStream_t s,
                       double *elapsed_ms);
 int mf_solver_labels_run(mf_matrix_s *A, int *vis, int nseg);
+int mf_spmm_run(mf_matrix_s *A, const double *d_X, double *d_Y, int tensor_cores, cudaStream_t s,
+                double *elapsed_ms);
 int mf_spmv_noalloc_run(mf_matrix_s *A, const double *d_x, double *d_y, int precision, cudaStream_t s);
 int mf_ref_labels_run(const double *d_pold, const double *d_pnew, int nseg, int *d_vis,
                       cudaStream_t s);

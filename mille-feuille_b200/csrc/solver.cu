@@ -644,7 +644,7 @@ __device__ __forceinline__ signed char rank_to_vis(int rank)
 
 // (int8_t) of a double as the x86-64 host compiler emits it (truncate to int32,
 // 0x80000000 when NaN / out of range, keep the low byte) -- the reference
-// converts p this way (main-cg-mixed.cu:464).
+// converts p this way (main-cg-mixed.cu:435).
 __device__ __forceinline__ int8_t trunc_i8(double v)
 {
     int w;
@@ -1432,6 +1432,44 @@ __device__ void grid_collect_m(const MultiParams &M, SharedM &sh, int kind, unsi
     __syncthreads();
 }
 
+// One chunk of the NR-column walk: lane i's stored values of the chunk at
+// entry offset cb in precision PR (FP32 / FP16 / scaled INT8 widened to FP64
+// against the FP64 operand rows, as the single-column walk: no FP32 copy of
+// R), each times its gathered NR-wide operand row.  The values are loaded one
+// at a time next to their use: the NR-wide accumulators and operand rows take
+// the registers, and these solves wait on the operand rows, not the values.
+template <int PR, int NR>
+__device__ __forceinline__ void multi_chunk(const SolverParams &P, long long cb, int i, unsigned hmask, int xb, int k0,
+                                            int len, float sc, const double *X64, double (&acc)[NR])
+{
+    const unsigned long long m8 = __ldcs((const unsigned long long *)(P.meta + cb) + i);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+        const int slot = (int)(mm >> 4);
+        const int xi = __shfl_sync(hmask, xb, slot, 16) + (int)(mm & 15u);
+        const float s8 = (PR == MF_P8) ? __shfl_sync(hmask, sc, slot, 16) : 0.0f;
+        if (k0 + j < len) {
+            double a;
+            if (PR == MF_P64) a = __ldcs(P.v64 + mf_slot<8>(cb, j, i));
+            else if (PR == MF_P32) a = (double)__ldcs(P.v32 + mf_slot<4>(cb, j, i));
+            else if (PR == MF_P16) a = (double)__half2float(P.v16[mf_slot<2>(cb, j, i)]);
+            else a = (double)((float)P.v8[mf_slot<1>(cb, j, i)] * s8);
+            if constexpr (NR == 1) {
+                acc[0] = fma(a, X64[xi], acc[0]);
+            } else {
+                const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
+#pragma unroll
+                for (int q = 0; q < NR / 2; q++) {
+                    const double2 d = xr[q];
+                    acc[2 * q] = fma(a, d.x, acc[2 * q]);
+                    acc[2 * q + 1] = fma(a, d.y, acc[2 * q + 1]);
+                }
+            }
+        }
+    }
+}
+
 // Y = A X for NR interleaved columns over the half-warp's slices; epi(R, acc)
 // once per tile-row with lane i's NR row sums.  Precision per slice as in
 // slice_dot (mixed: from the column segments' max over rows and columns).
@@ -1472,38 +1510,12 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
         const long long off = hdr_off(h);
         for (int k0 = 0; k0 < kp; k0 += 8) {
             const long long cb = off + (long long)(k0 >> 3) * 128;
-            double v64[8];
-            float vf[8];
-            // stored FP32 / FP16 / scaled-INT8 values are widened to FP64 against
-            // the FP64 operand rows (as the single-column walk): no FP32 copy of R
-            if (!kMixed || pr == MF_P64) load_chunk<MF_P64>(P, cb, i, len - k0, v64, vf);
-            else if (pr == MF_P32) load_chunk<MF_P32>(P, cb, i, len - k0, v64, vf);
-            else if (pr == MF_P16) load_chunk<MF_P16>(P, cb, i, len - k0, v64, vf);
-            else load_chunk<MF_P8>(P, cb, i, len - k0, v64, vf);
-            const unsigned long long m8 = __ldcs((const unsigned long long *)(P.meta + cb) + i);
-#pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
-                const int slot = (int)(mm >> 4);
-                const int xi = __shfl_sync(hmask, xb, slot, 16) + (int)(mm & 15u);
-                const float s8 = (kMixed && pr == MF_P8) ? __shfl_sync(hmask, sc, slot, 16) : 0.0f;
-                if (k0 + j < len) {
-                    const double v = (!kMixed || pr == MF_P64) ? v64[j]
-                                     : (pr == MF_P8)           ? (double)(vf[j] * s8)
-                                                               : (double)vf[j];
-                    if constexpr (NR == 1) {
-                        acc[0] = fma(v, X64[xi], acc[0]);
-                    } else {
-                        const double2 *xr = (const double2 *)(X64 + (long long)xi * NR);
-#pragma unroll
-                        for (int q = 0; q < NR / 2; q++) {
-                            const double2 d = xr[q];
-                            acc[2 * q] = fma(v, d.x, acc[2 * q]);
-                            acc[2 * q + 1] = fma(v, d.y, acc[2 * q + 1]);
-                        }
-                    }
-                }
-            }
+            // one instantiation per stored precision, so only that precision's
+            // values are live across the chunk's gathers
+            if (!kMixed || pr == MF_P64) multi_chunk<MF_P64, NR>(P, cb, i, hmask, xb, k0, len, sc, X64, acc);
+            else if (pr == MF_P32) multi_chunk<MF_P32, NR>(P, cb, i, hmask, xb, k0, len, sc, X64, acc);
+            else if (pr == MF_P16) multi_chunk<MF_P16, NR>(P, cb, i, hmask, xb, k0, len, sc, X64, acc);
+            else multi_chunk<MF_P8, NR>(P, cb, i, hmask, xb, k0, len, sc, X64, acc);
         }
         if (hdr_last(h)) {
             epi(h.y, acc);
@@ -2646,6 +2658,168 @@ int mf_ref_labels_run(const double *d_pold, const double *d_pnew, int nseg, int 
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaStreamSynchronize(s));
     return MF_SUCCESS;
+}
+
+// ------------------------------------------------------------ tensor-core experiment (8 right-hand sides)
+// Y = A X for 8 interleaved columns (row i's 8 values contiguous) with every
+// tile's values stored in FP16, in two forms:
+//  * CUDA cores (k_spmm_cc): the solver's arithmetic -- a half-warp per
+//    tile-row, the FP16 value widened to FP64 against the FP64 row of X, 8
+//    FP64 sums per row;
+//  * tensor cores (k_spmm_tc): a warp per tile-row; each 16 x 16 tile of a
+//    slice is densified in shared memory from the sparse payload (nothing
+//    dense is read from HBM), X's 16 x 8 segment is rounded to FP16, and one
+//    mma.sync.m16n8k16 per tile accumulates the 16 x 8 block in FP32.
+// Both read the same slice payload; mf_debug_spmm times them side by side.
+namespace {
+__global__ void k_interleave(const double *B, int n, int L, int nrhs, int g, int NR, double *Bi);
+__global__ void k_deinterleave(const double *Xi, int n, int nrhs, int g, int NR, double *X);
+
+constexpr int kTcWarps = 4;                          // warps per block of k_spmm_tc
+constexpr int kTcSmem = kTcWarps * MF_SEG_TILES * 256 * 2;   // dense FP16 tiles of one slice per warp
+
+__global__ void __launch_bounds__(kThreads, 2) k_spmm_cc(SolverParams P, const double *X, double *Y)
+{
+    const int lane = threadIdx.x & 31, i = lane & 15;
+    const unsigned hmask = 0xFFFFu << (16 * (lane >> 4));
+    const int R = ((blockIdx.x * blockDim.x + threadIdx.x) >> 4);
+    if (R >= P.tilem) return;
+    double acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) acc[q] = 0.0;
+    for (int s = P.seg_ptr[R]; s < P.seg_ptr[R + 1]; s++) {
+        const int4 h = P.seg_hdr[s];
+        const int xb = (P.seg_tile[(long long)s * MF_BS + i] >> 8) * MF_BS;
+        const int len = P.seg_rowlen[(long long)s * MF_BS + i];
+        for (int k0 = 0; k0 < hdr_kp(h); k0 += 8) {
+            const long long cb = hdr_off(h) + (long long)(k0 >> 3) * 128;
+            double v64[8];
+            float v[8];
+            load_chunk<MF_P16>(P, cb, i, len - k0, v64, v);
+            const unsigned long long m8 = __ldcs((const unsigned long long *)(P.meta + cb) + i);
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+                const int xi = __shfl_sync(hmask, xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
+                if (k0 + j < len) {
+                    const double2 *xr = (const double2 *)(X + (long long)xi * 8);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const double2 d = xr[q];
+                        acc[2 * q] = fma((double)v[j], d.x, acc[2 * q]);
+                        acc[2 * q + 1] = fma((double)v[j], d.y, acc[2 * q + 1]);
+                    }
+                }
+            }
+        }
+    }
+    const int row = R * MF_BS + i;
+    if (row < P.n) {
+        double2 *yr = (double2 *)(Y + (long long)row * 8);
+#pragma unroll
+        for (int q = 0; q < 4; q++) yr[q] = make_double2(acc[2 * q], acc[2 * q + 1]);
+    }
+}
+
+__device__ __forceinline__ unsigned pack_half2(double lo, double hi)
+{
+    return (unsigned)__half_as_ushort(__double2half(lo)) | ((unsigned)__half_as_ushort(__double2half(hi)) << 16);
+}
+
+__global__ void __launch_bounds__(kTcWarps * 32) k_spmm_tc(SolverParams P, const double *X, double *Y)
+{
+    extern __shared__ __align__(16) unsigned short tc_tiles[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int R = blockIdx.x * kTcWarps + w;
+    if (R >= P.tilem) return;
+    unsigned short *tiles = tc_tiles + w * MF_SEG_TILES * 256;   // [slot][row][col] FP16 bits
+    const int g = lane >> 2, c = lane & 3;
+    float d[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int s = P.seg_ptr[R]; s < P.seg_ptr[R + 1]; s++) {
+        const int4 h = P.seg_hdr[s];
+        const int nt = hdr_nt(h);
+        for (int e = lane; e < nt * 128; e += 32) ((unsigned *)tiles)[e] = 0u;
+        __syncwarp();
+        // lanes 0..15 scatter their row's entries into the dense tiles
+        if (lane < 16) {
+            const int len = P.seg_rowlen[(long long)s * MF_BS + lane];
+            for (int k0 = 0; k0 < len; k0 += 8) {
+                const long long cb = hdr_off(h) + (long long)(k0 >> 3) * 128;
+                const uint4 u = __ldcs((const uint4 *)(P.v16 + cb) + lane);
+                const unsigned long long m8 = __ldcs((const unsigned long long *)(P.meta + cb) + lane);
+                const unsigned wv[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    if (k0 + j >= len) break;
+                    const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+                    tiles[(mm >> 4) * 256 + lane * 16 + (mm & 15u)] =
+                        (unsigned short)((wv[j >> 1] >> (16 * (j & 1))) & 0xFFFFu);
+                }
+            }
+        }
+        __syncwarp();
+        const int tw = (lane < nt) ? P.seg_tile[(long long)s * MF_BS + lane] : 0;
+        for (int t = 0; t < nt; t++) {
+            const int xb = (__shfl_sync(0xffffffffu, tw, t) >> 8) * MF_BS;
+            const unsigned *T32 = (const unsigned *)(tiles + t * 256);
+            // A (16 x 16, row-major) fragment of m16n8k16
+            const unsigned a0 = T32[(g * 16 + 2 * c) >> 1], a1 = T32[((g + 8) * 16 + 2 * c) >> 1];
+            const unsigned a2 = T32[(g * 16 + 2 * c + 8) >> 1], a3 = T32[((g + 8) * 16 + 2 * c + 8) >> 1];
+            // B (16 x 8) fragment: X rows xb + k, column g, rounded to FP16
+            const double *xr = X + (long long)xb * 8 + g;
+            const unsigned b0 = pack_half2(xr[(2 * c) * 8], xr[(2 * c + 1) * 8]);
+            const unsigned b1 = pack_half2(xr[(2 * c + 8) * 8], xr[(2 * c + 9) * 8]);
+            asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                         "{%8, %9}, {%0, %1, %2, %3};"
+                         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+        }
+        __syncwarp();
+    }
+    const int r0 = R * MF_BS + g, r1 = r0 + 8;
+    if (r0 < P.n) *(double2 *)(Y + (long long)r0 * 8 + 2 * c) = make_double2(d[0], d[1]);
+    if (r1 < P.n) *(double2 *)(Y + (long long)r1 * 8 + 2 * c) = make_double2(d[2], d[3]);
+}
+}  // namespace
+
+// Y = A X for 8 right-hand sides with FP16 stored values (the columns of X
+// and Y one after another, n_cols / n_rows each); tensor_cores selects
+// k_spmm_tc over k_spmm_cc.  elapsed_ms: the kernel alone.
+int mf_spmm_run(mf_matrix_s *A, const double *d_X, double *d_Y, int tensor_cores, cudaStream_t s,
+                double *elapsed_ms)
+{
+    Workspace *w = nullptr;
+    MF_TRY(ws_get(A, 0, &w, s));
+    const long long L = A->vec_len;
+    double *Xi = nullptr, *Yi = nullptr;
+    MF_TRY(dal(&Xi, L * 8));
+    MF_TRY(dal(&Yi, L * 8));
+    int rc = MF_SUCCESS;
+    do {
+        if (cudaMemsetAsync(Xi, 0, (size_t)L * 8 * sizeof(double), s) != cudaSuccess) { rc = MF_ERR_CUDA; break; }
+        k_interleave<<<592, 256, 0, s>>>(d_X, A->n_cols, (int)L, 8, 0, 8, Xi);
+        SolverParams P;
+        fill_params(P, A, w);
+        if (cudaEventRecord(w->e0, s) != cudaSuccess) { rc = MF_ERR_CUDA; break; }
+        if (tensor_cores) {
+            if (cudaFuncSetAttribute(k_spmm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem) != cudaSuccess) {
+                rc = MF_ERR_CUDA;
+                break;
+            }
+            k_spmm_tc<<<(A->tilem + kTcWarps - 1) / kTcWarps, kTcWarps * 32, kTcSmem, s>>>(P, Xi, Yi);
+        } else {
+            k_spmm_cc<<<(A->tilem * 16 + kThreads - 1) / kThreads, kThreads, 0, s>>>(P, Xi, Yi);
+        }
+        if (cudaGetLastError() != cudaSuccess || cudaEventRecord(w->e1, s) != cudaSuccess) { rc = MF_ERR_CUDA; break; }
+        k_deinterleave<<<592, 256, 0, s>>>(Yi, A->n_rows, 8, 0, 8, d_Y);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) { rc = MF_ERR_CUDA; break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, w->e0, w->e1);
+        if (elapsed_ms) *elapsed_ms = ms;
+    } while (0);
+    cudaFree(Xi);
+    cudaFree(Yi);
+    return rc;
 }
 
 // ------------------------------------------------------------ allocation-free SpMV

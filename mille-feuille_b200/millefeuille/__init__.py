@@ -201,6 +201,25 @@ class Matrix:
         check(_lib.load().mf_debug_spmv_tiles(self._h, _ptr(x), _ptr(y), int(tile_prec), 0), "mf_debug_spmv_tiles")
         return y
 
+    def spmm8(self, X, tensor_cores=False):
+        """Experiment hook (mf_debug_spmm): Y = A X for 8 right-hand sides (rows
+        of X, shape (8, n_cols)) with FP16 stored values, on the CUDA cores or
+        the tensor cores.  Returns (Y, kernel ms).  Host arrays or CUDA tensors."""
+        dev = _is_cuda_tensor(X)
+        if dev:
+            import torch
+            X = X.contiguous()
+            Y = torch.empty((8, self.info["n_rows"]), dtype=torch.float64, device=X.device)
+        else:
+            X = np.ascontiguousarray(X, dtype=np.float64)
+            Y = np.zeros((8, self.info["n_rows"]), dtype=np.float64)
+        if tuple(X.shape) != (8, self.info["n_cols"]):
+            raise ValueError("spmm8 takes X of shape (8, n_cols)")
+        ms = C.c_double()
+        check(_lib.load().mf_debug_spmm(self._h, _ptr(X), _ptr(Y), int(bool(tensor_cores)), int(dev), C.byref(ms)),
+              "mf_debug_spmm")
+        return Y, ms.value
+
     def solver_labels(self):
         """Test hook (mf_debug_solver_labels): the labels the last parity-mode
         solve left for the next SpMV, one per column segment (d_vis codes)."""

@@ -73,7 +73,7 @@ EXPORTED = [
     "mf_debug_ref_labels", "mf_build_arch", "mf_spmv_noalloc", "mf_value_grad", "mf_matrix_create_transposed",
     "mf_solve_multi", "mf_batch_create", "mf_batch_tune", "mf_batch_solve", "mf_batch_destroy",
     "mf_batch_partition", "mf_batch_schedule", "mf_debug_spmv_tiles", "mf_debug_solver_labels",
-    "mf_dropin_last_report",
+    "mf_dropin_last_report", "mf_debug_spmm",
 ]
 
 _lib = None
@@ -113,6 +113,7 @@ def load() -> C.CDLL:
     L.mf_debug_spmv_tiles.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.mf_debug_solver_labels.argtypes = [vp, vp, C.c_int]
     L.mf_dropin_last_report.argtypes = [C.POINTER(Report)]
+    L.mf_debug_spmm.argtypes = [vp, vp, vp, C.c_int, C.c_int, dp]
     L.mf_read_matrix.argtypes = [C.c_char_p, ip, ip, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(dp), ip]
     L.mf_write_cbd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, vp, vp, vp]
     L.mf_free_host.argtypes = [vp]

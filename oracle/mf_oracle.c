@@ -672,7 +672,7 @@ static double dot_seq(int n, const double *a, const double *b)
  * per iteration: q = A p with the label-selected tile arithmetic, alpha =
  * r.r / p.q, r -= alpha q, beta = r'.r' / r.r, x += alpha p, p = r + beta p;
  * then p's shadows (float)p, half(p) (__double2half, one rounding) and
- * (int8_t)p (the int8 conversion of main-cg-mixed.cu:434) and the labels of
+ * (int8_t)p (the int8 conversion of main-cg-mixed.cu:435) and the labels of
  * the next SpMV from |p_new - p_old| per 16-element segment (thresholds of
  * main-cg-mixed.cu:1334-1351).  The reference keeps the class of whichever
  * lane wrote last; here the most conservative class wins (one of the
