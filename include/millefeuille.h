@@ -35,7 +35,9 @@ typedef enum {
     MF_ERR_UNSUPPORTED = 5,    /* input outside the supported envelope */
     MF_ERR_BREAKDOWN = 6,      /* a Krylov scalar became 0 / non-finite */
     MF_ERR_IO = 7,             /* matrix file could not be read */
-    MF_ERR_NOT_BUILT = 8       /* no CUDA device available */
+    MF_ERR_NOT_BUILT = 8,      /* no CUDA device available */
+    MF_ERR_CHECK = 9           /* bounds-checked build only: a kernel index failed its bounds check
+                                  (the access was skipped; site, index and limit go to stderr) */
 } mf_status;
 
 const char *mf_status_string(int status);
@@ -149,6 +151,11 @@ typedef struct {
                               test keep the final accuracy).  0 = off */
     int relax_int8;        /* with relax_eta: the relaxed precision may go down to scaled INT8
                               (default 0: FP16 at most) */
+    int test_check_limit;  /* test hook of the bounds-checked build (libmillefeuille_check.so), mf_solve
+                              only: the kernels check the operand's gathered entries against this
+                              length (rounded down to a multiple of 16) instead of the padded vector
+                              length, so the check path runs without any out-of-bounds index.  0 = off;
+                              the normal build ignores it */
 } mf_options;
 
 typedef struct {

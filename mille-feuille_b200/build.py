@@ -10,18 +10,27 @@ solver of main-cg.cu).  The drop-in driver executables (main-cg, main-cg-mixed,
 main-bicg, main-bicg-mixed) go to mille-feuille_b200/bin/, main-cg linked
 against the FP64 variant (all git-ignored, carried with the tree).  Rebuilds
 only what changed.
+
+    python mille-feuille_b200/build.py --check
+
+also builds libmillefeuille_check.so: solver.cu and api.cu compiled with
+MF_CHECK, every kernel index taken from stored data checked against its
+array's extent (MF_ERR_CHECK on a failed check; the access is skipped).  Load
+it with MILLEFEUILLE_LIB=<path> in place of libmillefeuille.so.
 """
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "millefeuille", "libmillefeuille.so")
 OUT_FP64 = os.path.join(HERE, "millefeuille", "libmillefeuille_fp64.so")
+OUT_CHECK = os.path.join(HERE, "millefeuille", "libmillefeuille_check.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 NVCC = os.environ.get("NVCC", "nvcc")
@@ -63,18 +72,30 @@ def _link(out: str, objs) -> None:
             raise RuntimeError(f"link failed: {os.path.basename(out)}")
 
 
-def build(verbose: bool = False) -> str:
+def build(verbose: bool = False, check: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     deps = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "millefeuille.h")]
-    objs = []
+    jobs, objs = [], []                  # (source, object, defines)
     for src in SOURCES:
         obj = os.path.join(BUILD, src + ".o")
         objs.append(obj)
-        _compile(os.path.join(CSRC, src), obj, deps, verbose)
+        jobs.append((src, obj, ()))
     api_fp64 = os.path.join(BUILD, "api_fp64.cu.o")
-    _compile(os.path.join(CSRC, "api.cu"), api_fp64, deps, verbose, defines=("MF_CG_INC_FP64",))
+    jobs.append(("api.cu", api_fp64, ("MF_CG_INC_FP64",)))
+    swap = {}
+    if check:
+        for src in ("solver.cu", "api.cu"):
+            obj = os.path.join(BUILD, src.replace(".cu", "_check.cu.o"))
+            swap[src + ".o"] = obj
+            jobs.append((src, obj, ("MF_CHECK",)))
+    # the translation units compile independently: one nvcc per core
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_compile, os.path.join(CSRC, src), obj, deps, verbose, d) for src, obj, d in jobs]:
+            f.result()
     _link(OUT, objs)
     _link(OUT_FP64, [api_fp64 if o.endswith("api.cu.o") else o for o in objs])
+    if check:
+        _link(OUT_CHECK, [swap.get(os.path.basename(o), o) for o in objs])
     build_drivers(verbose)
     return OUT
 
@@ -104,4 +125,4 @@ def build_drivers(verbose: bool = False) -> None:
 
 
 if __name__ == "__main__":
-    print(build(verbose="--verbose" in sys.argv))
+    print(build(verbose="--verbose" in sys.argv, check="--check" in sys.argv))

@@ -50,11 +50,14 @@ const char *mf_status_string(int status)
     case MF_ERR_BREAKDOWN: return "Krylov breakdown (zero or non-finite scalar)";
     case MF_ERR_IO: return "matrix file could not be read";
     case MF_ERR_NOT_BUILT: return "no CUDA device available";
+    case MF_ERR_CHECK: return "a kernel index failed its bounds check (bounds-checked build)";
     default: return "unknown status";
     }
 }
 
-#ifdef MF_CG_INC_FP64
+#if defined(MF_CHECK)
+const char *mf_build_arch(void) { return "sm_100a (bounds-checked)"; }
+#elif defined(MF_CG_INC_FP64)
 const char *mf_build_arch(void) { return "sm_100a (cg_solve_inc: FP64, main-cg.cu)"; }
 #else
 const char *mf_build_arch(void) { return "sm_100a"; }

@@ -9,12 +9,15 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmillefeuille.so")
+# MILLEFEUILLE_LIB selects another build of the same ABI, e.g. the
+# bounds-checked libmillefeuille_check.so (build.py --check)
+LIB_PATH = os.environ.get("MILLEFEUILLE_LIB") or os.path.join(HERE, "libmillefeuille.so")
+LIB_CHECK_PATH = os.path.join(HERE, "libmillefeuille_check.so")
 # the same library with cg_solve_inc in FP64 (main-cg.cu's entry point)
 LIB_FP64_PATH = os.path.join(HERE, "libmillefeuille_fp64.so")
 
 MF_SUCCESS, MF_ERR_INVALID, MF_ERR_CUDA, MF_ERR_NOMEM, MF_ERR_TIMEOUT = 0, 1, 2, 3, 4
-MF_ERR_UNSUPPORTED, MF_ERR_BREAKDOWN, MF_ERR_IO, MF_ERR_NOT_BUILT = 5, 6, 7, 8
+MF_ERR_UNSUPPORTED, MF_ERR_BREAKDOWN, MF_ERR_IO, MF_ERR_NOT_BUILT, MF_ERR_CHECK = 5, 6, 7, 8, 9
 MF_METHOD_CG, MF_METHOD_BICGSTAB = 0, 1
 MF_PREC_FP64, MF_PREC_MIXED, MF_PREC_PARITY = 0, 1, 2
 
@@ -31,7 +34,7 @@ class Options(C.Structure):
                 ("demote_int8", C.c_double), ("use_lossless", C.c_int), ("wait_timeout_s", C.c_double),
                 ("blocks_per_sm", C.c_int), ("threads_per_block", C.c_int), ("x0_given", C.c_int),
                 ("l2_window", C.c_int), ("test_stall_barrier", C.c_int), ("demote_min_fraction", C.c_double),
-                ("relax_eta", C.c_double), ("relax_int8", C.c_int)]
+                ("relax_eta", C.c_double), ("relax_int8", C.c_int), ("test_check_limit", C.c_int)]
 
 
 class Report(C.Structure):

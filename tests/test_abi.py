@@ -38,7 +38,7 @@ def test_status_strings_and_defaults(mf):
     from millefeuille import _lib
     L = _lib.load()
     assert L.mf_build_arch().decode() == "sm_100a"
-    for s in range(0, 9):
+    for s in range(0, 10):
         assert len(_lib.status_string(s)) > 3
     o = mf.default_options()
     assert o.precision == mf.MF_PREC_MIXED and o.replace_every == 50 and o.tol == 1e-8
@@ -47,6 +47,24 @@ def test_status_strings_and_defaults(mf):
     # the ctypes mirror of mf_options has the C layout: the last field is set by mf_options_default
     assert o.demote_min_fraction == 0.125 and o.x0_given == 0 and o.l2_window == 1 and o.use_lossless == 1
     assert o.demote_fp16 == 2.0 ** -13 and o.demote_int8 == 2.0 ** -16 and o.wait_timeout_s == 10.0
+
+
+def test_checked_build_loads_and_exports_the_same_symbols(mf):
+    """libmillefeuille_check.so (build.py --check) has the normal build's ABI."""
+    from millefeuille import _lib
+    if not os.path.exists(_lib.LIB_CHECK_PATH):
+        import importlib
+        importlib.import_module("build").build(check=True)
+    L = C.CDLL(_lib.LIB_CHECK_PATH)
+    missing = [n for n in _declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    L.mf_build_arch.restype = C.c_char_p
+    assert L.mf_build_arch().decode() == "sm_100a (bounds-checked)"
+    L.mf_status_string.restype = C.c_char_p
+    assert b"bounds check" in L.mf_status_string(9)
+    o = _lib.Options()
+    L.mf_options_default(C.byref(o))
+    assert o.test_check_limit == 0 and o.relax_int8 == 0 and o.demote_min_fraction == 0.125
 
 
 def test_no_device_reports_not_built(mf):

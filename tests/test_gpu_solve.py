@@ -85,8 +85,28 @@ def test_gpu_cg_mixed_converges_fp64_verified(mf, oracle_mod, cuda, p3d):
     assert _relres(A, x, b) <= 1.0001e-8
     T = oracle_mod.Tiles(A.n, A.n, A.rowptr, A.colidx, A.val)
     _, ro = T.cg_fp64(b, tol=1e-8, max_iter=10000)
-    assert rep["iterations"] <= 1.3 * ro["iterations"] + 5
+    # FP32-stored values cost a few iterations (measured 294 against 280 on this
+    # 32^3 system, 1,509 against 1,402 on 128^3)
+    assert rep["iterations"] <= 1.08 * ro["iterations"] + 3, (rep["iterations"], ro["iterations"])
     assert sum(rep["tile_uses"][1:]) > 0          # low-precision tiles were used
+
+
+def test_gpu_mixed_usage_counters_cover_every_entry(mf, cuda, p3d):
+    """The report's per-precision counters.  With every tile in FP32 (smooth
+    right-hand side, no tile exact in a narrower type), each mixed-mode SpMV
+    counts every tile and every stored entry once: the lean FP32 walk, which
+    reads no row lengths, takes its entry count from the CSR row pointers of
+    its tile-rows, and the totals must equal (SpMVs) x (tiles, nnz)."""
+    A, b, _ = p3d
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    x, rep = G.solve(b, method="cg", precision="mixed", tol=1e-8)
+    T = G.info["tilenum"]
+    tu, nu = rep["tile_uses"], rep["nnz_uses"]
+    assert tu[0] == tu[2] == tu[3] == 0 and nu[0] == nu[2] == nu[3] == 0, (tu, nu)
+    assert tu[1] % T == 0, (tu, T)
+    nspmv = tu[1] // T
+    assert nspmv >= rep["iterations"]
+    assert nu[1] == nspmv * A.nnz, (nu, nspmv, A.nnz)
 
 
 def test_gpu_mixed_demotes_small_segments_and_converges(mf, cuda, p3d):
@@ -101,6 +121,10 @@ def test_gpu_mixed_demotes_small_segments_and_converges(mf, cuda, p3d):
     x, rep = G.solve(b, method="cg", precision="mixed", tol=1e-8)
     assert rep["converged"] and _relres(A, x, b) <= 1.0001e-8
     assert rep["tile_uses"][2] + rep["tile_uses"][3] > 0, rep["tile_uses"]
+    # every SpMV counts each tile and each stored entry once, in the precision it ran
+    T = G.info["tilenum"]
+    assert sum(rep["tile_uses"]) % T == 0
+    assert sum(rep["nnz_uses"]) == sum(rep["tile_uses"]) // T * A.nnz, (rep["tile_uses"], rep["nnz_uses"])
     # demote_min_fraction = 1: narrower tiles only if every segment is small -> all FP32
     x1, rep1 = G.solve(b, method="cg", precision="mixed", tol=1e-8, demote_min_fraction=1.0)
     assert rep1["converged"] and _relres(A, x1, b) <= 1.0001e-8
