@@ -494,23 +494,39 @@ __device__ __forceinline__ int load_len(const SolverParams &P, int s, int i, int
     return chk_in(CHK_ROWLEN, len, hdr_kp(h) + 1) ? len : 0;
 }
 
-// Mixed mode when no tile can leave FP32 in this SpMV: every slice runs the
-// FP32 chunk loop directly (no per-slice precision reduction); the range's tile
-// and entry totals go to the counters once, at the end.
-// Lane i's FP32 values and index word of the chunk at entry offset cb
-// (unpredicated: the stored padding past a row's end is zero).
-__device__ __forceinline__ void load_chunk_f32(const SolverParams &P, long long cb, int i, float4 &a, float4 &b,
-                                               unsigned long long &m)
-{
-    a = __ldcs((const float4 *)(P.v32 + cb) + i);
-    b = __ldcs((const float4 *)(P.v32 + cb + 64) + i);
-    m = __ldcs((const unsigned long long *)(P.meta + cb) + i);
-}
+// One chunk of the lean walk: lane i's 8 stored values of a uniform-precision
+// slice (FP32: two 16-byte loads) and its index word, loaded unpredicated (the
+// stored padding past a row's end is zero).  The same pipelined walk over FP64
+// slices (four 16-byte loads per chunk) measured no faster than
+// slice_dot_uniform on the 128^3 FP64 solve and SpMV, so FP64 keeps that.
+template <int PR> struct LeanChunk;
 
-// Mixed mode when no tile can leave FP32 in this SpMV: every slice runs FP32
-// stored values (no per-slice precision reduction); the range's tile and
-// entry totals go to the counters once, at the end (entries from the CSR row
-// pointers of the range's tile-rows).
+template <> struct LeanChunk<MF_P32> {
+    float4 a, b;
+    unsigned long long m;
+    __device__ __forceinline__ void zero()
+    {
+        a = b = make_float4(0.f, 0.f, 0.f, 0.f);
+        m = 0ull;
+    }
+    __device__ __forceinline__ void load(const SolverParams &P, long long cb, int i)
+    {
+        a = __ldcs((const float4 *)(P.v32 + cb) + i);
+        b = __ldcs((const float4 *)(P.v32 + cb + 64) + i);
+        m = __ldcs((const unsigned long long *)(P.meta + cb) + i);
+    }
+    __device__ __forceinline__ void values(double (&v)[8]) const
+    {
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    }
+};
+
+// The lean walk: every slice of the range runs stored precision PR (mixed mode
+// when no tile can leave FP32 in this SpMV, and the standalone FP32 SpMV), no
+// per-slice precision reduction; the range's tile and entry totals go to the
+// counters once, at the end (entries from the CSR row pointers of the range's
+// tile-rows).
 // The walk reads no row lengths: a row's padding entries are stored as value
 // 0 with index byte 0 (slot 0, column 0), so for them a lane gathers x at the
 // slice's first tile column and adds 0 * x.  Without the per-lane row-length
@@ -522,9 +538,9 @@ __device__ __forceinline__ void load_chunk_f32(const SolverParams &P, long long 
 // gathers are issued, so their DRAM trip overlaps chunk c's gathers, sum and
 // tile-row epilogue instead of following them.  Sums are formed in the same
 // order as slice_dot_uniform (per slice from 0, added to the tile-row's sum).
-template <typename Epi>
-__device__ __forceinline__ void spmv_range_f32(const SolverParams &P, int sb, int se, int i, unsigned hmask,
-                                               const XVec &X, unsigned *cnt, Epi &epi)
+template <int PR, typename Epi>
+__device__ __forceinline__ void spmv_range_lean(const SolverParams &P, int sb, int se, int i, unsigned hmask,
+                                                const XVec &X, unsigned *cnt, Epi &epi)
 {
     int4 h = P.seg_hdr[sb];
     const int4 hl = P.seg_hdr[se - 1];
@@ -534,9 +550,8 @@ __device__ __forceinline__ void spmv_range_f32(const SolverParams &P, int sb, in
         return;
     const int R0 = h.y;
     int tw = load_tw(P, sb, i);
-    float4 a, b;
-    unsigned long long m8;
-    load_chunk_f32(P, off0, i, a, b, m8);
+    LeanChunk<PR> cur;
+    cur.load(P, off0, i);
     int4 hn = make_int4(0, 0, 0, 0);
     int twn = 0;
     int s = sb, kc = 0, kchunks = hdr_kp(h) >> 3;
@@ -551,16 +566,17 @@ __device__ __forceinline__ void spmv_range_f32(const SolverParams &P, int sb, in
         double xv[8];
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            const unsigned mm = (unsigned)(m8 >> (8 * j)) & 0xFFu;
+            const unsigned mm = (unsigned)(cur.m >> (8 * j)) & 0xFFu;
             const int xi = __shfl_sync(hmask, xb, (int)(mm >> 4), 16) + (int)(mm & 15u);
             xv[j] = chk_in(CHK_X, xi, P.chk_xlen) ? X.x64[xi] : 0.0;
         }
-        float4 an = make_float4(0.f, 0.f, 0.f, 0.f), bn = an;
-        unsigned long long mn = 0ull;
-        if (c + 1 < nch) load_chunk_f32(P, off0 + (long long)(c + 1) * 128, i, an, bn, mn);
-        const float v[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+        LeanChunk<PR> nxt;
+        nxt.zero();
+        if (c + 1 < nch) nxt.load(P, off0 + (long long)(c + 1) * 128, i);
+        double v[8];
+        cur.values(v);
 #pragma unroll
-        for (int j = 0; j < 8; j++) sacc = fma((double)v[j], xv[j], sacc);
+        for (int j = 0; j < 8; j++) sacc = fma(v[j], xv[j], sacc);
         if (++kc == kchunks) {             // the slice is done
             ntiles += (unsigned)hdr_nt(h);
             acc += sacc;
@@ -575,13 +591,11 @@ __device__ __forceinline__ void spmv_range_f32(const SolverParams &P, int sb, in
             kc = 0;
             kchunks = hdr_kp(h) >> 3;
         }
-        a = an;
-        b = bn;
-        m8 = mn;
+        cur = nxt;
     }
     if (cnt && i == 0 && chk_in(CHK_ROW, R0, P.tilem) && chk_in(CHK_ROW, hl.y, P.tilem)) {
-        cnt[MF_P32] += ntiles;
-        cnt[5 + MF_P32] += (unsigned)(P.rowptr[min(P.n, (hl.y + 1) * MF_BS)] - P.rowptr[R0 * MF_BS]);
+        cnt[PR] += ntiles;
+        cnt[5 + PR] += (unsigned)(P.rowptr[min(P.n, (hl.y + 1) * MF_BS)] - P.rowptr[R0 * MF_BS]);
     }
 }
 
@@ -602,8 +616,8 @@ __device__ __forceinline__ void spmv_range(const SolverParams &P, int sb, int se
 {
     if (sb >= se) return;
     if (!chk_in(CHK_SLICE, sb, P.nseg) || !chk_in(CHK_SLICE, se - 1, P.nseg)) return;
-    if (MODE == MODE_MIXED && !F64 && !X.dyn && X.force_pr < 0) {
-        spmv_range_f32(P, sb, se, i, hmask, X, cnt, epi);
+    if (MODE == MODE_MIXED && !F64 && ((!X.dyn && X.force_pr < 0) || X.force_pr == MF_P32)) {
+        spmv_range_lean<MF_P32>(P, sb, se, i, hmask, X, cnt, epi);
         return;
     }
     // row lengths: parity mode only (its tile arithmetic walks real entries)
@@ -913,6 +927,14 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 ((mx <= 0.0 || -neg_mn <= (double)P.demote16 * mx) && nsmall >= (double)P.min_small)) ? 1 : 0;
     };
     int dynA = (MODE == MODE_MIXED) ? dyn_of(v[1], v[2], v[3]) : 0;
+    // mixed CG: the x / r update records r's per-segment magnitudes (one
+    // half-warp max reduction and one store per tile-row, 4.5 % of the 128^3
+    // solve) only while enough segments were small in the last update that the
+    // next SpMV may demote tiles; otherwise it keeps just r's maximum and the
+    // count of small segments (a vote per tile-row), and the next SpMV runs
+    // all-FP32.  Demotion then starts one update after the small segments do.
+    const float half_small = 0.5f * fmaxf(1.0f, P.min_small);
+    int magB = (MODE == MODE_MIXED) ? ((P.lossless_any || v[3] >= (double)half_small) ? 1 : 0) : 1;
             clk.lap(PH_BAR);
     const double bb = P.x0_given ? bb0 : v[0];
     double rr = v[0], r1 = v[0];
@@ -1001,8 +1023,14 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                         P.r[row] = rn;
                         prr += rn * rn;
                     }
-                    publish_dir<MODE>(R, row, valid, rn, 0.0, nullptr, nullptr, nullptr, P.mag_r, nullptr, rmax,
-                                      c.hmask, false, &rmin, rthr, &rsm);
+                    if (MODE != MODE_MIXED || magB) {
+                        publish_dir<MODE>(R, row, valid, rn, 0.0, nullptr, nullptr, nullptr, P.mag_r, nullptr, rmax,
+                                          c.hmask, false, &rmin, rthr, &rsm);
+                    } else {
+                        const float m = valid ? (float)fabs(rn) : 0.0f;
+                        rmax = fmaxf(rmax, m);
+                        if (__all_sync(c.hmask, m <= rthr) && c.i == 0) rsm += 1.0f;
+                    }
                 }
             }
             clk.lap(PH_VECB);
@@ -1013,7 +1041,10 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             double rr_new = v[0];
             const double rr_rec = rr_new;       // recursive r.r of this iteration
             invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
-            if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2], v[3]);
+            if (MODE == MODE_MIXED) {
+                dynA = magB ? dyn_of(v[1], v[2], v[3]) : 0;
+                magB = (P.lossless_any || v[3] >= (double)half_small) ? 1 : 0;
+            }
             k++;
             last_true = 0;
             const bool want_check = !P.fixed_iters && rr_new <= thr2;
@@ -1060,7 +1091,10 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 clk.lap(PH_BAR);
                 rr_new = v[0];
                 invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
-                if (MODE == MODE_MIXED) dynA = dyn_of(v[1], v[2], v[3]);
+                if (MODE == MODE_MIXED) {
+                    dynA = dyn_of(v[1], v[2], v[3]);     // the replacement records every segment
+                    magB = (P.lossless_any || v[3] >= (double)half_small) ? 1 : 0;
+                }
                 rr_true = rr_new;
                 repl++;
                 last_true = 1;
@@ -1510,7 +1544,7 @@ __device__ __forceinline__ void multi_chunk(const SolverParams &P, long long cb,
         const int slot = (int)(mm >> 4);
         const int xi = __shfl_sync(hmask, xb, slot, 16) + (int)(mm & 15u);
         const float s8 = (PR == MF_P8) ? __shfl_sync(hmask, sc, slot, 16) : 0.0f;
-        if (k0 + j < len && chk_in(CHK_X, xi, P.chk_xlen)) {
+        if ((NR < 8 || k0 + j < len) && chk_in(CHK_X, xi, P.chk_xlen)) {
             double a;
             if (PR == MF_P64) a = __ldcs(P.v64 + mf_slot<8>(cb, j, i));
             else if (PR == MF_P32) a = (double)__ldcs(P.v32 + mf_slot<4>(cb, j, i));
@@ -1534,12 +1568,17 @@ __device__ __forceinline__ void multi_chunk(const SolverParams &P, long long cb,
 // Y = A X for NR interleaved columns over the half-warp's slices; epi(R, acc)
 // once per tile-row with lane i's NR row sums.  Precision per slice as in
 // slice_dot (mixed: from the column segments' max over rows and columns).
+// Up to 4 columns the walk reads no row lengths (padding is value 0 with
+// index byte 0, as in slice_dot_uniform: measured 10 % faster on the
+// 512-system batch); with 8 columns a padding entry would gather 64 bytes of
+// X, and the row-length predicate measured 6 % faster on the 512^2 system.
 template <int MODE, int NR, bool F64, typename Epi>
 __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se, int i, unsigned hmask,
                                            const double *X64, const float *mag, float invM,
                                            int dyn, Epi epi)
 {
     constexpr bool kMixed = (MODE == MODE_MIXED) && !F64;
+    constexpr bool kLen = NR >= 8;
     XVec X = make_x(X64, nullptr, nullptr, nullptr, mag, nullptr, invM, dyn);
     double acc[NR];
 #pragma unroll
@@ -1548,7 +1587,7 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
     if (!chk_in(CHK_SLICE, sb, P.nseg) || !chk_in(CHK_SLICE, se - 1, P.nseg)) return;
     int4 h = P.seg_hdr[sb];
     int tw = load_tw(P, sb, i);
-    int len = load_len(P, sb, i, h);
+    int len = kLen ? load_len(P, sb, i, h) : 0;
     for (int s = sb; s < se; s++) {
         const bool more = s + 1 < se;
         int4 hn = make_int4(0, 0, 0, 0);
@@ -1556,7 +1595,7 @@ __device__ __forceinline__ void spmv_multi(const SolverParams &P, int sb, int se
         if (more) {
             hn = P.seg_hdr[s + 1];
             twn = load_tw(P, s + 1, i);
-            lenn = load_len(P, s + 1, i, hn);
+            lenn = kLen ? load_len(P, s + 1, i, hn) : 0;
         }
         const int xb = (tw >> 8) * MF_BS;
         int pr = MF_P64;
@@ -3688,10 +3727,13 @@ int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cud
         if (rc != MF_SUCCESS) break;
         if (cl[1] == 2 && B.max_res[2] < 1) continue;
         if ((rc = batch_build_items(B, cl[0], cl[1], run)) != MF_SUCCESS) break;
-        double ms = 0.0;
-        for (int rep = 0; rep < 2 && rc == MF_SUCCESS; rep++) {   // the first run warms up
+        // the first run warms up; the faster of the next two counts (one timed
+        // run of 20 iterations picked two blocks per SM where one was 7 %
+        // faster over the whole 512-system batch)
+        double ms = 1e300;
+        for (int rep = 0; rep < 3 && rc == MF_SUCCESS; rep++) {
             rc = mf_batch_solve_impl(b, bufB.data(), bufX.data(), &o, nullptr, 0, run);
-            ms = B.last_ms;
+            if (rep > 0) ms = std::min(ms, B.last_ms);
         }
         if (rc == MF_SUCCESS && ms < best_ms) {
             best_ms = ms;
