@@ -130,9 +130,8 @@ typedef struct {
     int blocks_per_sm;     /* 0: from occupancy */
     int threads_per_block; /* 0: default (512) */
     int x0_given;          /* 1: x holds the initial guess on entry (mf_solve: CG and BiCGSTAB, every
-                              precision; mf_solve_multi: X, every column; the first residual
-                              r = b - A x is formed in FP64).  mf_batch_solve returns
-                              MF_ERR_UNSUPPORTED for it */
+                              precision; mf_solve_multi and mf_batch_solve: X, every column; the
+                              first residual r = b - A x is formed in FP64) */
     int l2_window;         /* 1 (default): keep the solver vectors in L2 with a persisting
                               access-policy window on the stream during the solve */
     int test_stall_barrier;/* test hook: 1 = the first grid barrier waits for one arrival that

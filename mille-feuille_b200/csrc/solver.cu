@@ -34,6 +34,7 @@ constexpr int kRedKinds = 10;     // reduction slot groups
 constexpr int kRedWidth = 4;      // doubles per group per block
 constexpr int kDefaultLB = 2;     // default register-budget variant of the persistent kernel
 constexpr int kVB = 4;            // tile-rows per step in the vector phases (loads in flight)
+constexpr int kDemoteCool = 16;   // SpMVs without per-slice lookups after one that did not pay
 
 enum { MODE_FP64 = 0, MODE_MIXED = 1, MODE_PARITY = 2 };
 
@@ -102,6 +103,8 @@ struct SolverParams {
     int method, max_iter, fixed_iters, replace_every, use_lossless;
     int x0_given;                 // x holds the initial guess: r = b - A x at the start
     int lossless_any;             // use_lossless and enough tiles are exact in INT8 / FP16
+    float min_demoted;            // mixed: a dynamic SpMV that runs fewer tiles than this below FP32
+                                  // turns the operand's per-slice lookups off for kDemoteCool SpMVs
     float min_small;              // mixed: narrower tiles only when at least this many column
                                   // segments were small in the operand's previous update
     double tol;
@@ -840,7 +843,11 @@ __device__ __forceinline__ int relaxed_precision(const SolverParams &P, double r
     return MF_P32;
 }
 
-template <int MODE, int LB>
+// METH: MF_METHOD_CG or MF_METHOD_BICGSTAB.  One instantiation per method, so
+// each gets its own register allocation: the kernel sits at the 64-register
+// limit of two 512-thread blocks per SM, and code in one method's branch
+// moves spills into the other's hot loop.
+template <int MODE, int LB, int METH>
 __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
 {
     __shared__ Shared sh;
@@ -855,7 +862,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     PhaseClock clk;
     clk.start(&sh);
     const int n = P.n;
-    const bool bicg = (P.method == MF_METHOD_BICGSTAB);
+    constexpr bool bicg = (METH == MF_METHOD_BICGSTAB);
 
     // ---- init: x = 0 (owned rows), r = b, p = r (rh = r) ----
     // With an initial guess: r = b - A x in FP64, and |b|^2 reduced on its own
@@ -927,6 +934,19 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 ((mx <= 0.0 || -neg_mn <= (double)P.demote16 * mx) && nsmall >= (double)P.min_small)) ? 1 : 0;
     };
     int dynA = (MODE == MODE_MIXED) ? dyn_of(v[1], v[2], v[3]) : 0;
+    // Feedback on the per-slice lookups (mixed): each SpMV's reduction also
+    // carries how many tiles it ran below FP32.  A dynamic SpMV that demoted
+    // fewer than min_demoted (demote_min_fraction of the tiles) did not pay
+    // for its lookups, and the same operand's next kDemoteCool SpMVs run the
+    // lean all-FP32 walk.  (A slice demotes only when all of its tiles'
+    // segments are small: on the 96^3 BiCGSTAB system 1.3 % of the tile
+    // products ran below FP32 while the lookups cost 7 % of the solve.)
+    constexpr int kNvFb = (MODE == MODE_MIXED) ? 2 : 1;
+    auto demoted = [&]() -> unsigned { return (MODE == MODE_MIXED && c.i == 0) ? cnt[MF_P16] + cnt[MF_P8] : 0u; };
+    auto next_cool = [&](int cool, bool was_dyn, double dem) -> int {
+        return cool > 0 ? cool - 1 : (was_dyn && dem < (double)P.min_demoted) ? kDemoteCool : 0;
+    };
+    int coolA = 0, coolS = 0;
     // mixed CG: the x / r update records r's per-segment magnitudes (one
     // half-warp max reduction and one store per tile-row, 4.5 % of the 128^3
     // solve) only while enough segments were small in the last update that the
@@ -962,8 +982,10 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             // ---- A: w = A r; p = r + beta p; q = w + beta q; p.q ----
             // (mixed: with a relaxed precision prA the whole SpMV runs in it)
             double ppq = 0.0;
-            XVec XA = make_x(P.r, nullptr, nullptr, nullptr, P.mag_r, nullptr, invM, dynA);
+            const int useA = (MODE == MODE_MIXED && coolA > 0) ? 0 : dynA;
+            XVec XA = make_x(P.r, nullptr, nullptr, nullptr, P.mag_r, nullptr, invM, useA);
             if (MODE == MODE_MIXED && prA != MF_P32) XA.force_pr = prA;
+            const unsigned d0A = demoted();
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask, XA, cnt, [&](int R, double y) {
                 const int row = R * MF_BS + c.i;
                 if (row < n) {
@@ -989,10 +1011,11 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             }
             nspmv++;
             clk.lap(PH_SPMV);
-            block_partial(P, sh, 1, ppq, 0, 0, 0, 1, 0u);
+            block_partial(P, sh, 1, ppq, (double)(demoted() - d0A), 0, 0, kNvFb, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 1, 1, 0u, v);
+            grid_collect(P, sh, 1, kNvFb, 0u, v);
             clk.lap(PH_BAR);
+            if (MODE == MODE_MIXED) coolA = next_cool(coolA, useA && XA.force_pr < 0, v[1]);
             const double alpha2 = rr / v[0];
             if (!isfinite(alpha2)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B: x += alpha p; r -= alpha q; r.r; r's shadow ----
@@ -1156,8 +1179,10 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
         } else {
             // ---- BiCGSTAB A1: v = A p, alpha = r1 / (rh.v) ----
             double prv = 0.0;
+            const int useA = (MODE == MODE_MIXED && coolA > 0) ? 0 : dynA;
+            const unsigned d0A = demoted();
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
-                             make_x(P.p, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, invM, dynA), cnt,
+                             make_x(P.p, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, invM, useA), cnt,
                              [&](int R, double y) {
                                  const int row = R * MF_BS + c.i;
                                  if (row < n) {
@@ -1167,10 +1192,11 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                              });
             nspmv++;
             clk.lap(PH_SPMV);
-            block_partial(P, sh, 1, prv, 0, 0, 0, 1, 0u);
+            block_partial(P, sh, 1, prv, (double)(demoted() - d0A), 0, 0, kNvFb, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 1, 1, 0u, v);
+            grid_collect(P, sh, 1, kNvFb, 0u, v);
             clk.lap(PH_BAR);
+            if (MODE == MODE_MIXED) coolA = next_cool(coolA, useA != 0, v[1]);
             alpha = r1 / v[0];
             if (!isfinite(alpha)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B1: s = r - alpha v ----
@@ -1198,8 +1224,10 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             const int dynS = (MODE == MODE_MIXED) ? dyn_of(v[0], v[1], v[2]) : 1;
             // ---- A2: t = A s, omega = (t.s)/(t.t) ----
             double pts = 0.0, ptt = 0.0;
+            const int useS = (MODE == MODE_MIXED && coolS > 0) ? 0 : dynS;
+            const unsigned d0S = demoted();
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
-                             make_x(P.s, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, invMs, dynS), cnt,
+                             make_x(P.s, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, invMs, useS), cnt,
                              [&](int R, double y) {
                                  const int row = R * MF_BS + c.i;
                                  if (row < n) {
@@ -1210,10 +1238,11 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                              });
             nspmv++;
             clk.lap(PH_SPMV);
-            block_partial(P, sh, 3, pts, ptt, 0, 0, 2, 0u);
+            block_partial(P, sh, 3, pts, ptt, (double)(demoted() - d0S), 0, kNvFb + 1, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 3, 2, 0u, v);
+            grid_collect(P, sh, 3, kNvFb + 1, 0u, v);
             clk.lap(PH_BAR);
+            if (MODE == MODE_MIXED) coolS = next_cool(coolS, useS != 0, v[2]);
             omega = (v[1] != 0.0) ? v[0] / v[1] : 0.0;
             // ---- B2: x += alpha p + omega s; r = s - omega t ----
             double prr = 0.0, prh = 0.0;
@@ -2063,6 +2092,7 @@ struct BatchParams {
     int *err;                     // first error of a team wait (zeroed before the launch)
     unsigned long long timeout_ns, arrive_timeout_ns;
     int stall_first;              // test hook: a team's first barrier expects one extra arrival
+    int x0_given;                 // every item's X holds its initial guess
     int max_iter, fixed_iters, replace_every, use_lossless;
     double tol, min_fraction;
     float demote16, demote8;
@@ -2223,7 +2253,7 @@ __device__ __forceinline__ SolverParams item_params(const BatchItem &it, const B
     P.v8 = it.v8;
     P.i8_scale = it.i8_scale;
     P.max_iter = B.max_iter;
-    P.x0_given = 0;
+    P.x0_given = B.x0_given;
     P.fixed_iters = B.fixed_iters;
     P.replace_every = B.replace_every;
     P.use_lossless = B.use_lossless;
@@ -2404,16 +2434,23 @@ inline int lossless_on(int use_lossless, double min_fraction, long long n_exact,
     return (use_lossless && n_exact > 0 && (double)n_exact >= min_fraction * (double)tilenum) ? 1 : 0;
 }
 
-const void *solve_kernel(int mode, int lb)
+template <int METH>
+const void *solve_kernel_m(int mode, int lb)
 {
     if (lb == 2) {
-        if (mode == MODE_FP64) return (const void *)k_solve<MODE_FP64, 2>;
-        if (mode == MODE_MIXED) return (const void *)k_solve<MODE_MIXED, 2>;
-        return (const void *)k_solve<MODE_PARITY, 2>;
+        if (mode == MODE_FP64) return (const void *)k_solve<MODE_FP64, 2, METH>;
+        if (mode == MODE_MIXED) return (const void *)k_solve<MODE_MIXED, 2, METH>;
+        return (const void *)k_solve<MODE_PARITY, 2, METH>;
     }
-    if (mode == MODE_FP64) return (const void *)k_solve<MODE_FP64, 1>;
-    if (mode == MODE_MIXED) return (const void *)k_solve<MODE_MIXED, 1>;
-    return (const void *)k_solve<MODE_PARITY, 1>;
+    if (mode == MODE_FP64) return (const void *)k_solve<MODE_FP64, 1, METH>;
+    if (mode == MODE_MIXED) return (const void *)k_solve<MODE_MIXED, 1, METH>;
+    return (const void *)k_solve<MODE_PARITY, 1, METH>;
+}
+
+const void *solve_kernel(int mode, int lb, int method)
+{
+    return method == MF_METHOD_BICGSTAB ? solve_kernel_m<MF_METHOD_BICGSTAB>(mode, lb)
+                                        : solve_kernel_m<MF_METHOD_CG>(mode, lb);
 }
 
 int ws_get(mf_matrix_s *A, int blocks_per_sm, Workspace **out, cudaStream_t s)
@@ -2430,9 +2467,11 @@ int ws_get(mf_matrix_s *A, int blocks_per_sm, Workspace **out, cudaStream_t s)
     // one grid size for every precision mode, so the cached workspace is shared
     int occ = 1 << 20;
     for (int m = MODE_FP64; m <= MODE_PARITY; m++) {
-        int o = 0;
-        MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, solve_kernel(m, lb), kThreads, 0));
-        occ = o < occ ? o : occ;
+        for (int meth = MF_METHOD_CG; meth <= MF_METHOD_BICGSTAB; meth++) {
+            int o = 0;
+            MF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, solve_kernel(m, lb, meth), kThreads, 0));
+            occ = o < occ ? o : occ;
+        }
     }
     if (occ < 1) return MF_ERR_UNSUPPORTED;
     if (occ > lb) occ = lb;
@@ -2672,6 +2711,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
     P.use_lossless = opt->use_lossless;
     P.lossless_any = lossless_on(opt->use_lossless, opt->demote_min_fraction, A->n_exact, A->tilenum);
     P.min_small = (float)(opt->demote_min_fraction * (double)A->tilem);
+    P.min_demoted = (float)(opt->demote_min_fraction * (double)A->tilenum);
     P.relax_eta = (float)opt->relax_eta;
     P.relax_int8 = opt->relax_int8 ? 1 : 0;
     P.fp16_ok = A->n_fp16_ok == A->tilenum ? 1 : 0;
@@ -2695,7 +2735,7 @@ int mf_solver_run(mf_matrix_s *A, const double *d_b, double *d_x, const mf_optio
                             : opt->method == MF_METHOD_BICGSTAB ? w->bicg_bytes : w->cg_bytes);
     const auto t_prepared = std::chrono::steady_clock::now();
     MF_CUDA_TRY(cudaEventRecord(w->e0, s));
-    cudaError_t lerr = cudaLaunchCooperativeKernel(solve_kernel(mode, w->lb), dim3(w->G), dim3(kThreads), args, 0, s);
+    cudaError_t lerr = cudaLaunchCooperativeKernel(solve_kernel(mode, w->lb, opt->method), dim3(w->G), dim3(kThreads), args, 0, s);
     if (lerr != cudaSuccess) {
         win.reset(s);
         MF_CUDA_TRY(lerr);
@@ -3163,6 +3203,7 @@ int mf_solver_multi_run(mf_matrix_s *A, int nrhs, const double *d_B, double *d_X
     P.use_lossless = opt->use_lossless;
     P.lossless_any = lossless_on(opt->use_lossless, opt->demote_min_fraction, A->n_exact, A->tilenum);
     P.min_small = (float)(opt->demote_min_fraction * (double)A->tilem);
+    P.min_demoted = (float)(opt->demote_min_fraction * (double)A->tilenum);
     P.tol = opt->tol;
     P.demote16 = (float)opt->demote_fp16;
     P.demote8 = (float)opt->demote_int8;
@@ -3451,6 +3492,9 @@ int batch_enqueue(BatchImpl &B, const double *const *Bd, double *const *Xd, cons
         const int nr = B.it_nr[t], g = B.it_col0[t] / nr;
         k_interleave<<<148, 256, 0, s>>>(Bd[B.it_sys[t]], A->n_rows, A->vec_len, B.nrhs[B.it_sys[t]], g, nr,
                                           (double *)B.h_items[t].M.B);
+        if (bp0.x0_given)          // the initial guesses: R = B - A X is formed in the launch
+            k_interleave<<<148, 256, 0, s>>>(Xd[B.it_sys[t]], A->n_rows, A->vec_len, B.nrhs[B.it_sys[t]], g, nr,
+                                              B.h_items[t].M.X);
     }
     MF_CUDA_TRY(cudaGetLastError());
     MF_CUDA_TRY(cudaMemsetAsync(B.d_ctl, 0, B.ctl_bytes, s));
@@ -3576,7 +3620,7 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
                         mf_report *reps, int use_graph, cudaStream_t s)
 {
     BatchImpl &B = b->impl;
-    if (opt->method != MF_METHOD_CG || opt->precision == MF_PREC_PARITY || opt->x0_given) return MF_ERR_UNSUPPORTED;
+    if (opt->method != MF_METHOD_CG || opt->precision == MF_PREC_PARITY) return MF_ERR_UNSUPPORTED;
     const int mode = opt->precision == MF_PREC_FP64 ? MODE_FP64 : MODE_MIXED;
     BatchParams bp;
     memset(&bp, 0, sizeof(bp));
@@ -3586,6 +3630,7 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
     bp.use_lossless = opt->use_lossless;
     bp.tol = opt->tol;
     bp.min_fraction = opt->demote_min_fraction;
+    bp.x0_given = opt->x0_given ? 1 : 0;
     bp.demote16 = (float)opt->demote_fp16;
     bp.demote8 = (float)opt->demote_int8;
     // team waits: within an item the members run in step (the normal bound);
@@ -3616,7 +3661,8 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
         const double opts[] = {opt->tol, (double)opt->max_iter, (double)opt->fixed_iters, (double)opt->replace_every,
                                opt->demote_fp16, opt->demote_int8, (double)opt->use_lossless, (double)B.cap,
                                (double)B.lb,
-                               opt->wait_timeout_s, (double)opt->test_stall_barrier, opt->demote_min_fraction};
+                               opt->wait_timeout_s, (double)opt->test_stall_barrier, opt->demote_min_fraction,
+                               (double)opt->x0_given};
         for (double v : opts) {
             unsigned long long u;
             memcpy(&u, &v, sizeof(u));

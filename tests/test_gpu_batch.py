@@ -145,3 +145,30 @@ def test_batch_team_wait_timeout_is_reported(mf, cuda):
         Xk = Xk.cpu().numpy()
         for c in range(B.shape[0]):
             assert rk[c]["converged"] and _relres(A, Xk[c], B[c]) <= 1.0001e-8
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 1e-8)])
+def test_batch_initial_guess(mf, cuda, systems, precision, tol):
+    """x0_given: every column starts from the X passed in (R = B - A X formed in
+    FP64 inside the launch).  From converged solutions no iteration runs; from
+    a 20-iteration start every column converges in fewer iterations than from
+    zero and to the same tolerance, with and without graph replay."""
+    mats, Bs = _setup(mf, systems)
+    batch = mf.Batch(mats, [B.shape[0] for B in Bs])
+    X1, r1 = batch.solve(Bs, method="cg", precision="fp64", tol=1e-10, use_graph=False)
+    X2, r2 = batch.solve(Bs, [x.clone() for x in X1], method="cg", precision=precision, tol=tol, x0_given=1,
+                         use_graph=False)
+    for rk in r2:
+        for col in rk:
+            assert col["converged"] and col["iterations"] <= 1, col
+    Xh, _ = batch.solve(Bs, method="cg", precision="fp64", max_iter=20, fixed_iters=1, use_graph=False)
+    for graph in (False, True):
+        X3, r3 = batch.solve(Bs, [x.clone() for x in Xh], method="cg", precision=precision, tol=tol, x0_given=1,
+                             use_graph=graph)
+        for (kind, side, A, B), X, rk, rk0 in zip(systems, X3, r3, r1):
+            X = X.cpu().numpy()
+            for c in range(B.shape[0]):
+                assert rk[c]["converged"] and rk[c]["relres_true"] <= tol, (kind, side, c, rk[c])
+                assert _relres(A, X[c], B[c]) <= tol * 1.0001
+                if rk0[c]["iterations"] > 25:
+                    assert rk[c]["iterations"] < rk0[c]["iterations"], (rk[c]["iterations"], rk0[c]["iterations"])
