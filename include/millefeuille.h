@@ -254,7 +254,9 @@ int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_o
  *                  batch) and sizes the work items (cap 8, one block per SM).
  * mf_batch_tune    picks the right-hand sides per item and the blocks per SM
  *                  ((8,1), (4,1), (2,1), (4,2), (2,2)) by timing `iters` fixed
- *                  iterations of the real batch; *chosen_cap (nullable) gets
+ *                  iterations of the real batch (two blocks per SM count 15 %
+ *                  slower than timed: the short probe favours them over a
+ *                  full solve's tail of long items); *chosen_cap (nullable) gets
  *                  the right-hand sides per item (grid_blocks in the reports
  *                  shows the blocks).
  * mf_batch_solve   B[k] / X[k]: DEVICE arrays of nrhs[k] x n_k doubles (one

@@ -608,11 +608,11 @@ __device__ __forceinline__ void spmv_range_lean(const SolverParams &P, int sb, i
 //
 // Descriptor pipeline: a half-warp's slices are stored back to back, so slice
 // s+1 starts where slice s ends (offset + 16 * kp).  The words indexed by the
-// slice number alone (header, lane i's tile word and row length) are loaded one
-// slice ahead, at the top of the previous slice, together with that slice's own
-// loads; the precision statistic (mixed / parity) is loaded one slice ahead
-// once the tile word is in.  A slice then waits for two round trips: values +
-// index word, then the gathered x.
+// slice number alone (header, lane i's tile word, and in parity mode its row
+// length) are loaded one slice ahead, at the top of the previous slice,
+// together with that slice's own loads; the precision statistic (mixed /
+// parity) is loaded one slice ahead once the tile word is in.  A slice then
+// waits for two round trips: values + index word, then the gathered x.
 template <int MODE, bool F64, typename Epi>
 __device__ __forceinline__ void spmv_range(const SolverParams &P, int sb, int se, int i, unsigned hmask,
                                            const XVec &X, unsigned *cnt, Epi epi)
@@ -951,8 +951,10 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
     // half-warp max reduction and one store per tile-row, 4.5 % of the 128^3
     // solve) only while enough segments were small in the last update that the
     // next SpMV may demote tiles; otherwise it keeps just r's maximum and the
-    // count of small segments (a vote per tile-row), and the next SpMV runs
-    // all-FP32.  Demotion then starts one update after the small segments do.
+    // count of small segments (a vote per tile-row, on every 4th update only:
+    // 1.5 % of the solve when taken on every one), and the next SpMV runs
+    // all-FP32.  Demotion then starts up to four updates after the small
+    // segments do.
     const float half_small = 0.5f * fmaxf(1.0f, P.min_small);
     int magB = (MODE == MODE_MIXED) ? ((P.lossless_any || v[3] >= (double)half_small) ? 1 : 0) : 1;
             clk.lap(PH_BAR);
@@ -1022,6 +1024,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             double prr = 0.0;
             float rmax = 0.0f, rmin = 3.0e38f, rsm = 0.0f;
             const float rthr = invM > 0.0f ? P.demote16 / invM : -1.0f;
+            const bool voteB = magB || (k & 3) == 0;     // this update counts small segments
             // kVB tile-rows per step: all loads first, so kVB round trips overlap
             for (int R0 = c.rbeg; R0 < c.rend; R0 += kVB) {
                 double xv[kVB], pv[kVB], rv[kVB], qv[kVB];
@@ -1052,7 +1055,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                     } else {
                         const float m = valid ? (float)fabs(rn) : 0.0f;
                         rmax = fmaxf(rmax, m);
-                        if (__all_sync(c.hmask, m <= rthr) && c.i == 0) rsm += 1.0f;
+                        if (voteB && __all_sync(c.hmask, m <= rthr) && c.i == 0) rsm += 1.0f;
                     }
                 }
             }
@@ -1066,7 +1069,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             invM = v[1] > 0.0 ? (float)(1.0 / v[1]) : 0.0f;
             if (MODE == MODE_MIXED) {
                 dynA = magB ? dyn_of(v[1], v[2], v[3]) : 0;
-                magB = (P.lossless_any || v[3] >= (double)half_small) ? 1 : 0;
+                if (voteB) magB = (P.lossless_any || v[3] >= (double)half_small) ? 1 : 0;
             }
             k++;
             last_true = 0;
@@ -3781,8 +3784,15 @@ int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cud
             rc = mf_batch_solve_impl(b, bufB.data(), bufX.data(), &o, nullptr, 0, run);
             if (rep > 0) ms = std::min(ms, B.last_ms);
         }
-        if (rc == MF_SUCCESS && ms < best_ms) {
-            best_ms = ms;
+        // Two blocks per SM (64 registers, the multi-column walk spills) win the
+        // short probe, where every item is active, but lose a full solve, whose
+        // end is a tail of a few long items run at per-block speed: on the
+        // 512-system batch the probe measured 315 ms (4 columns, 2 blocks)
+        // against 344 ms (4 columns, 1 block), and the whole solve 13.2 s
+        // against 11.2 s.  They count 15 % slower than measured.
+        const double score = cl[1] == 2 ? 1.15 * ms : ms;
+        if (rc == MF_SUCCESS && score < best_ms) {
+            best_ms = score;
             best = cl[0];
             best_lb = cl[1];
         }
