@@ -294,7 +294,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     if not args.no_c1:
-        out["config"]["laplace2d_256"] = c1_line(dev, args.steps)
+        out["config"]["laplace2d_256"] = laplace_line(dev, args.steps, 256, 1e-10)
+        out["config"]["laplace2d_2048"] = laplace_line(dev, args.steps, 2048, TOL)
     if not args.no_bicgstab:
         out["config"]["bicgstab"] = bicgstab_line(dev, args.steps)
     if not args.no_adjoint:
@@ -307,22 +308,25 @@ def run_ours(args, rank, world, local_rank):
         print(json.dumps(out), flush=True)
 
 
-def c1_line(dev, steps):
-    """The 2D 5-point Laplacian on 256^2 (n = 65,536; b = A x_true, x_true ~
-    U(-1,1) seed 0, x0 = 0): CG to 1e-10 in FP64 (max 10,000 iterations, the
-    plain-CG configuration) and in mixed precision.  About 4 MB of matrix per
-    SpMV sits in L2, so the solve is bound by the grid syncs: reported in us
-    per iteration.  One untimed solve each, then the best of `steps`."""
+def laplace_line(dev, steps, N=256, tol=1e-10):
+    """The 2D 5-point Laplacian on N^2 (b = A x_true, x_true ~ U(-1,1) seed 0,
+    x0 = 0): CG to tol in FP64 (max 10,000 iterations, the plain-CG
+    configuration) and in mixed precision.  Its values 4 and -1 are exact in
+    FP16, so the mixed mode streams FP16 values through the lookup-free walk.
+    N = 256 (C1): about 4 MB of matrix per SpMV sits in L2, so the solve is
+    bound by the grid syncs (reported in us per iteration); N = 2048: 21 M
+    entries, bound by the matrix stream.  One untimed solve each, then the best
+    of `steps`."""
     import torch
     import millefeuille as mf
     from millefeuille import matrices as M
-    A, b, xt = M.laplace2d_system(256, seed=0)
+    A, b, xt = M.laplace2d_system(N, seed=0)
     G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
     bd = torch.from_numpy(b).to(dev)
     xd = torch.zeros_like(bd)
-    out = {"workload": f"laplace2d_256 (n={A.n}, nnz={A.nnz}), CG tol 1e-10, max 10000 iterations"}
+    out = {"workload": f"laplace2d_{N} (n={A.n}, nnz={A.nnz}), CG tol {tol:g}, max 10000 iterations"}
     for prec in ("fp64", "mixed"):
-        o = mf.default_options(precision=prec, tol=1e-10, max_iter=10000, replace_every=0 if prec == "fp64" else 50)
+        o = mf.default_options(precision=prec, tol=tol, max_iter=10000, replace_every=0 if prec == "fp64" else 50)
         G.solve(bd, xd, options=o)
         best = None
         for _ in range(max(1, steps)):
@@ -331,9 +335,10 @@ def c1_line(dev, steps):
                 best = r
         d = {"ms": round(best["time_ms"], 3), "iterations": best["iterations"],
              "us_per_iteration": round(best["time_ms"] * 1e3 / max(1, best["iterations"]), 2),
-             "relres_true": best["relres_true"]}
+             "relres_true": best["relres_true"], "tile_uses": best["tile_uses"]}
         d.update(verify(A, xd.cpu().numpy(), b, xt))
         out[prec] = d
+    out["mixed_vs_fp64_speedup"] = round(out["fp64"]["ms"] / out["mixed"]["ms"], 3)
     return out
 
 

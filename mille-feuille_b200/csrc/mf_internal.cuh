@@ -100,6 +100,7 @@ struct mf_matrix_s {
     int n_exact_known;
     long long n_exact;
     long long n_fp16_ok;       // tiles whose values lie within FP16's normal range
+    long long n_exact_f16;     // tiles whose values FP16 reproduces exactly
 };
 
 // Position of entry k of row i in the slice whose payload starts at entry

@@ -308,3 +308,46 @@ def test_gpu_relaxed_precision_converges_and_uses_fp16(mf, cuda, p3d):
     assert rep["converged"] and rep["relres_true"] <= 1e-8
     assert _relres(A, x, b) <= 1.0001e-8
     assert rep["tile_uses"][2] > 0 and rep["tile_uses"][3] == 0, rep["tile_uses"]
+
+
+def test_gpu_demotion_feedback_turns_unpaid_lookups_off(mf, cuda):
+    """Mixed BiCGSTAB on a 48^3 convection-diffusion system: enough of the
+    operands' column segments are small that per-slice lookups engage, but a
+    slice demotes only when all of its tiles' segments are small, so each
+    dynamic SpMV runs few tiles below FP32.  The demotion feedback then turns
+    the lookups off for the next 16 SpMVs: the solve runs a small fraction of
+    the FP16 / INT8 tile products that the same solve with the gates off
+    (demote_min_fraction = 0: every SpMV dynamic) runs.  Both converge on the
+    FP64 true residual."""
+    from millefeuille import matrices as M
+    C, bc, _ = M.convdiff3d(48, seed=2)
+    G = mf.Matrix.from_csr(C.n, C.n, C.rowptr, C.colidx, C.val)
+    x1, r1 = G.solve(bc, method="bicgstab", precision="mixed", tol=1e-8)
+    x0, r0 = G.solve(bc, method="bicgstab", precision="mixed", tol=1e-8, demote_min_fraction=0.0)
+    for x, r in ((x1, r1), (x0, r0)):
+        assert r["converged"] and _relres(C, x, bc) <= 1.0001e-8, r
+    low1 = r1["tile_uses"][2] + r1["tile_uses"][3]
+    low0 = r0["tile_uses"][2] + r0["tile_uses"][3]
+    assert low0 > 1000 and 0 < low1 < 0.2 * low0, (r1["tile_uses"], r0["tile_uses"])
+
+
+def test_gpu_fp16_exact_matrix_runs_fp16_lean_walk(mf, cuda):
+    """Every tile of the 2D Laplacian (values 4 and -1) is exact in FP16, so the
+    mixed mode runs its SpMVs on FP16 stored values through the lookup-free
+    walk: no tile product runs in FP32 or FP64, each SpMV counts every tile and
+    entry once, and since the values lose nothing the solve takes the FP64
+    solve's iterations and agrees with its x.  use_lossless = 0 keeps FP32."""
+    from millefeuille import matrices as M
+    A, b, _ = M.laplace2d_system(96, seed=0)
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    xf, rf = G.solve(b, precision="fp64", tol=1e-10, replace_every=0)
+    xm, rm = G.solve(b, precision="mixed", tol=1e-10)
+    assert rm["converged"] and _relres(A, xm, b) <= 1.0001e-10, rm
+    T = G.info["tilenum"]
+    tu, nu = rm["tile_uses"], rm["nnz_uses"]
+    assert tu[0] == 0 and tu[1] == 0 and tu[2] > 0, tu
+    assert sum(tu) % T == 0 and sum(nu) == sum(tu) // T * A.nnz, (tu, nu)
+    assert abs(rm["iterations"] - rf["iterations"]) <= 2, (rm["iterations"], rf["iterations"])
+    np.testing.assert_allclose(xm, xf, rtol=0, atol=1e-8 * np.abs(xf).max())
+    x2, r2 = G.solve(b, precision="mixed", tol=1e-10, use_lossless=0)
+    assert r2["converged"] and r2["tile_uses"][2] == 0 and r2["tile_uses"][1] > 0, r2["tile_uses"]
