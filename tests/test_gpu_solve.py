@@ -351,3 +351,7 @@ def test_gpu_fp16_exact_matrix_runs_fp16_lean_walk(mf, cuda):
     np.testing.assert_allclose(xm, xf, rtol=0, atol=1e-8 * np.abs(xf).max())
     x2, r2 = G.solve(b, precision="mixed", tol=1e-10, use_lossless=0)
     assert r2["converged"] and r2["tile_uses"][2] == 0 and r2["tile_uses"][1] > 0, r2["tile_uses"]
+    # BiCGSTAB takes the same FP16 walk for both of its SpMVs
+    x3, r3 = G.solve(b, method="bicgstab", precision="mixed", tol=1e-10)
+    assert r3["converged"] and _relres(A, x3, b) <= 1.0001e-10, r3
+    assert r3["tile_uses"][0] == 0 and r3["tile_uses"][1] == 0 and r3["tile_uses"][2] > 0, r3["tile_uses"]
