@@ -971,15 +971,18 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
                 ((mx <= 0.0 || -neg_mn <= (double)P.demote16 * mx) && nsmall >= (double)P.min_small)) ? 1 : 0;
     };
     int dynA = (MODE == MODE_MIXED) ? dyn_of(v[1], v[2], v[3]) : 0;
-    // Feedback on the per-slice lookups (mixed): each SpMV's reduction also
-    // carries how many tiles it ran below FP32.  A dynamic SpMV that demoted
-    // fewer than min_demoted (demote_min_fraction of the tiles) did not pay
-    // for its lookups, and the same operand's next kDemoteCool SpMVs run the
-    // lean all-FP32 walk.  (A slice demotes only when all of its tiles'
+    // Feedback on the per-slice lookups (mixed BiCGSTAB): each SpMV's reduction
+    // also carries how many tiles it ran below FP32.  A dynamic SpMV that
+    // demoted fewer than min_demoted (demote_min_fraction of the tiles) did
+    // not pay for its lookups, and the same operand's next kDemoteCool SpMVs
+    // run the lean walk.  (A slice demotes only when all of its tiles'
     // segments are small: on the 96^3 BiCGSTAB system 1.3 % of the tile
-    // products ran below FP32 while the lookups cost 7 % of the solve.)
-    constexpr int kNvFb = (MODE == MODE_MIXED) ? 2 : 1;
-    auto demoted = [&]() -> unsigned { return (MODE == MODE_MIXED && c.i == 0) ? cnt[MF_P16] + cnt[MF_P8] : 0u; };
+    // products ran below FP32 while the lookups cost 7 % of the solve.)  CG
+    // goes without it: the extra reduction value and counters cost its mixed
+    // 128^3 solve 3.5 % although its lookups never engage there.
+    constexpr bool kFb = (MODE == MODE_MIXED) && bicg;
+    constexpr int kNvFb = kFb ? 2 : 1;
+    auto demoted = [&]() -> unsigned { return (kFb && c.i == 0) ? cnt[MF_P16] + cnt[MF_P8] : 0u; };
     auto next_cool = [&](int cool, bool was_dyn, double dem) -> int {
         return cool > 0 ? cool - 1 : (was_dyn && dem < (double)P.min_demoted) ? kDemoteCool : 0;
     };
@@ -1026,11 +1029,9 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             // ---- A: w = A r; p = r + beta p; q = w + beta q; p.q ----
             // (mixed: with a relaxed precision prA the whole SpMV runs in it)
             double ppq = 0.0;
-            const int useA = (MODE == MODE_MIXED && coolA > 0) ? 0 : dynA;
-            XVec XA = make_x(P.r, nullptr, nullptr, nullptr, P.mag_r, nullptr, invM, useA);
+            XVec XA = make_x(P.r, nullptr, nullptr, nullptr, P.mag_r, nullptr, invM, dynA);
             if (MODE == MODE_MIXED && prA != MF_P32) XA.force_pr = prA;
             if (P.lean_f16) XA.lean_pr = MF_P16;
-            const unsigned d0A = demoted();
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask, XA, cnt, [&](int R, double y) {
                 const int row = R * MF_BS + c.i;
                 if (row < n) {
@@ -1056,11 +1057,10 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             }
             nspmv++;
             clk.lap(PH_SPMV);
-            block_partial(P, sh, 1, ppq, (double)(demoted() - d0A), 0, 0, kNvFb, 0u);
+            block_partial(P, sh, 1, ppq, 0, 0, 0, 1, 0u);
             if (!grid_barrier(P, epoch, sh)) return;
-            grid_collect(P, sh, 1, kNvFb, 0u, v);
+            grid_collect(P, sh, 1, 1, 0u, v);
             clk.lap(PH_BAR);
-            if (MODE == MODE_MIXED) coolA = next_cool(coolA, useA && XA.force_pr < 0, v[1]);
             const double alpha2 = rr / v[0];
             if (!isfinite(alpha2)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B: x += alpha p; r -= alpha q; r.r; r's shadow ----
@@ -1225,7 +1225,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
         } else {
             // ---- BiCGSTAB A1: v = A p, alpha = r1 / (rh.v) ----
             double prv = 0.0;
-            const int useA = (MODE == MODE_MIXED && coolA > 0) ? 0 : dynA;
+            const int useA = (kFb && coolA > 0) ? 0 : dynA;
             const unsigned d0A = demoted();
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
                              lean_base(make_x(P.p, P.p32, P.p16, P.p8, P.mag_p, P.lab_p, invM, useA)), cnt,
@@ -1242,7 +1242,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 1, kNvFb, 0u, v);
             clk.lap(PH_BAR);
-            if (MODE == MODE_MIXED) coolA = next_cool(coolA, useA != 0, v[1]);
+            if (kFb) coolA = next_cool(coolA, useA != 0, v[1]);
             alpha = r1 / v[0];
             if (!isfinite(alpha)) { status = MF_ERR_BREAKDOWN; break; }
             // ---- B1: s = r - alpha v ----
@@ -1270,7 +1270,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             const int dynS = (MODE == MODE_MIXED) ? dyn_of(v[0], v[1], v[2]) : 1;
             // ---- A2: t = A s, omega = (t.s)/(t.t) ----
             double pts = 0.0, ptt = 0.0;
-            const int useS = (MODE == MODE_MIXED && coolS > 0) ? 0 : dynS;
+            const int useS = (kFb && coolS > 0) ? 0 : dynS;
             const unsigned d0S = demoted();
             spmv_range<MODE, false>(P, c.sbeg, c.send, c.i, c.hmask,
                              lean_base(make_x(P.s, P.s32, P.s16, P.s8, P.mag_s, P.lab_s, invMs, useS)), cnt,
@@ -1288,7 +1288,7 @@ __global__ void __launch_bounds__(kThreads, LB) k_solve(SolverParams P)
             if (!grid_barrier(P, epoch, sh)) return;
             grid_collect(P, sh, 3, kNvFb + 1, 0u, v);
             clk.lap(PH_BAR);
-            if (MODE == MODE_MIXED) coolS = next_cool(coolS, useS != 0, v[2]);
+            if (kFb) coolS = next_cool(coolS, useS != 0, v[2]);
             omega = (v[1] != 0.0) ? v[0] / v[1] : 0.0;
             // ---- B2: x += alpha p + omega s; r = s - omega t ----
             double prr = 0.0, prh = 0.0;
