@@ -502,11 +502,34 @@ __device__ __forceinline__ int load_len(const SolverParams &P, int s, int i, int
 }
 
 // One chunk of the lean walk: lane i's 8 stored values of a uniform-precision
-// slice (FP32: two 16-byte loads) and its index word, loaded unpredicated (the
-// stored padding past a row's end is zero).  The same pipelined walk over FP64
-// slices (four 16-byte loads per chunk) measured no faster than
-// slice_dot_uniform on the 128^3 FP64 solve and SpMV, so FP64 keeps that.
+// slice (FP64: four 16-byte loads; FP32: two; FP16: one) and its index word,
+// loaded unpredicated (the stored padding past a row's end is zero).
 template <int PR> struct LeanChunk;
+
+template <> struct LeanChunk<MF_P64> {
+    double2 d[4];
+    unsigned long long m;
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int q = 0; q < 4; q++) d[q] = make_double2(0.0, 0.0);
+        m = 0ull;
+    }
+    __device__ __forceinline__ void load(const SolverParams &P, long long cb, int i)
+    {
+#pragma unroll
+        for (int q = 0; q < 4; q++) d[q] = __ldcs((const double2 *)(P.v64 + cb + 32 * q) + i);
+        m = __ldcs((const unsigned long long *)(P.meta + cb) + i);
+    }
+    __device__ __forceinline__ void values(double (&v)[8]) const
+    {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            v[2 * q] = d[q].x;
+            v[2 * q + 1] = d[q].y;
+        }
+    }
+};
 
 template <> struct LeanChunk<MF_P32> {
     float4 a, b;
@@ -553,9 +576,9 @@ template <> struct LeanChunk<MF_P16> {
     }
 };
 
-// The lean walk: every slice of the range runs stored precision PR (mixed mode
-// when no tile can leave the base precision in this SpMV -- FP32, or FP16 when
-// every tile is exact in FP16 -- and the standalone FP32 / FP16 SpMVs), no
+// The lean walk: every slice of the range runs stored precision PR (the FP64
+// mode; mixed mode when no tile can leave the base precision in this SpMV --
+// FP32, or FP16 when every tile is exact in FP16; the standalone SpMVs), no
 // per-slice precision reduction; the range's tile and entry totals go to the
 // counters once, at the end (entries from the CSR row pointers of the range's
 // tile-rows).
@@ -648,6 +671,13 @@ __device__ __forceinline__ void spmv_range(const SolverParams &P, int sb, int se
 {
     if (sb >= se) return;
     if (!chk_in(CHK_SLICE, sb, P.nseg) || !chk_in(CHK_SLICE, se - 1, P.nseg)) return;
+    // the FP64 mode takes the pipelined walk too (128^3 FP64 CG 62.0 -> 60.3 ms);
+    // the mixed mode's FP64 replacement SpMVs do not: in that kernel the extra
+    // code cost the mixed solve more (61.3 -> 62.0 ms) than it saved
+    if (MODE == MODE_FP64) {
+        spmv_range_lean<MF_P64>(P, sb, se, i, hmask, X, cnt, epi);
+        return;
+    }
     if (MODE == MODE_MIXED && !F64) {
         const int lean = (X.force_pr < 0 && !X.dyn) ? X.lean_pr : X.force_pr;
         if (lean == MF_P32) {
