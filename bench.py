@@ -462,7 +462,8 @@ def fwd_adjoint(dev, nrhs):
         e2.record()
         torch.cuda.synchronize(dev)
         if timed:
-            adj_reps = pat.reports
+            # backward appends the adjoint solves' reports after the forward ones
+            adj_reps = pat.reports[len(fwd_reps):]
             fwd_ms, tot_ms = e0.elapsed_time(e1), e0.elapsed_time(e2)
             res = {"workload": f"aniso2d_grf_512 (n={A.n}, nnz={A.nnz}) x {nrhs} rhs, mixed CG tol 1e-8, "
                                "loss ||X - X_target||^2, grads for b and A's values",
