@@ -313,7 +313,7 @@ def laplace_line(dev, steps, N=256, tol=1e-10):
     x0 = 0): CG to tol in FP64 (max 10,000 iterations, the plain-CG
     configuration) and in mixed precision.  Its values 4 and -1 are exact in
     FP16, so the mixed mode streams FP16 values through the lookup-free walk.
-    N = 256 (C1): about 4 MB of matrix per SpMV sits in L2, so the solve is
+    N = 256: about 4 MB of matrix per SpMV sits in L2, so the solve is
     bound by the grid syncs (reported in us per iteration); N = 2048: 21 M
     entries, bound by the matrix stream.  One untimed solve each, then the best
     of `steps`."""

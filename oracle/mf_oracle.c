@@ -1,7 +1,7 @@
 /*
  * mf_oracle.c -- CPU restatement of Mille-feuille's tile path.
  *
- * TEST INFRASTRUCTURE ONLY (the checker).  Only tests/, smoke() and bench.py's
+ * TEST INFRASTRUCTURE ONLY (the test oracle).  Only tests/, smoke() and bench.py's
  * cpu_baseline / reference arm call this code.  The product never does.
  *
  * Each function names the reference file:line (inside the zhaijiaqi/Mille-feuille

@@ -1,7 +1,7 @@
 /*
  * mf_oracle.h -- CPU restatement of Mille-feuille's tile path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker: tests/, the
+ * TEST INFRASTRUCTURE ONLY.  This library is the test oracle: tests/, the
  * smoke() entry and bench.py's cpu_baseline / reference arm may call it.
  * The product (libmillefeuille.so) never links or calls it.
  *

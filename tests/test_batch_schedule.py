@@ -4,8 +4,8 @@
 The launch is cooperative (every block resident), and team members wait for
 each other at bounded barriers; the schedule must therefore never make two
 teams wait on each other: every block's list follows one global order of the
-team items.  These tests check that order and the sizing rules on the C4 list
-and on random cost sets."""
+team items.  These tests check that order and the sizing rules on the list of the
+512-system batch (seed 3) and on random cost sets."""
 import math
 
 import numpy as np
@@ -65,7 +65,7 @@ def _check(mf, cost, tilem, grid):
     return team, lists, queue
 
 
-def test_schedule_on_the_c4_list(mf):
+def test_schedule_on_the_512_system_batch(mf):
     from millefeuille import matrices as M
     cost, tilem = _item_costs(M.batch_specs(512, seed=3))
     for grid in (148, 296):
