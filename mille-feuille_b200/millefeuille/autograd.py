@@ -4,8 +4,11 @@ and for A's stored values.
     x = sparse_solve(rowptr, colidx, val, b, method="cg", precision="mixed")
     loss(x).backward()        # fills val.grad and b.grad
 
-Forward: the single-kernel solve on device pointers (mf_solve_multi, up to 8
-right-hand sides per launch, for CG; one mf_solve per column for BiCGSTAB).  Backward: the adjoint solve lambda = A^-T dL/dx with the same
+Forward: the single-kernel solve on device pointers -- for CG, mf_solve_multi
+(up to 8 right-hand sides in one launch) or, with more than 8, a one-system
+mf_batch tuned once per tiled handle and right-hand-side count (work items of
+up to 8 columns solved concurrently by teams of blocks); one mf_solve per
+column for BiCGSTAB.  Backward: the adjoint solve lambda = A^-T dL/dx with the same
 kernel -- on A itself for CG (A symmetric), on a transposed handle
 (mf_matrix_create_transposed) for BiCGSTAB -- then dL/db = lambda and
 dL/dval[e] = -sum_k lambda_k[i] x_k[j] over A's stored pattern (mf_value_grad,
@@ -20,7 +23,7 @@ from __future__ import annotations
 
 import torch
 
-from . import Matrix, default_options
+from . import Batch, Matrix, default_options
 
 
 class SolvePattern:
@@ -35,11 +38,13 @@ class SolvePattern:
         self._key = None
         self._A = None
         self._AT = None
+        self._batches = {}          # (handle, nrhs, precision) -> tuned one-system Batch
         self.reports = []           # per-solve reports of the last forward / backward
 
     def matrix(self, val) -> Matrix:
         key = (val.data_ptr(), val._version, tuple(val.shape))
         if self._A is None or key != self._key:
+            self.close_batches()
             self._A = Matrix.from_csr(self.n_rows, self.n_cols, self.rowptr, self.colidx, val.detach().contiguous())
             self._AT = None
             self._key = key
@@ -52,12 +57,43 @@ class SolvePattern:
             self._AT = self._A.transposed()
         return self._AT
 
+    def batch(self, A: Matrix, nrhs: int, precision: int, stream) -> Batch:
+        """The one-system batch of A with nrhs right-hand sides, created and
+        tuned (mf_batch_tune: columns per work item, blocks per SM) on first
+        use and kept until the values change."""
+        key = (id(A), int(nrhs), int(precision))
+        bt = self._batches.get(key)
+        if bt is None:
+            bt = Batch([A], [int(nrhs)], stream=stream)
+            bt.tune(int(precision), stream=stream)
+            self._batches[key] = bt
+        return bt
 
-def _solve_all(A: Matrix, B, opts, reports):
-    """All right-hand sides: mf_solve_multi (up to 8 per launch) for CG in the
-    FP64 / mixed modes, one mf_solve per column otherwise."""
+    def close_batches(self) -> None:
+        for bt in self._batches.values():
+            bt.close()
+        self._batches = {}
+
+
+# More right-hand sides than one multi-column launch takes: a one-system batch.
+# Its work items (up to 8 columns each) run concurrently on teams of blocks,
+# where mf_solve_multi would run one 8-column group after another on the
+# whole grid (32 columns of the 512^2 anisotropic system: 1.62 s against 2.0 s).
+_BATCH_ABOVE = 8
+
+
+def _solve_all(A: Matrix, B, opts, reports, pattern: "SolvePattern"):
+    """All right-hand sides: for CG in the FP64 / mixed modes, mf_solve_multi
+    (up to 8) or the pattern's tuned one-system batch (more than 8); one
+    mf_solve per column otherwise."""
     X = torch.zeros_like(B)
     if B.shape[0] > 1 and opts.method == 0 and opts.precision in (0, 1):
+        if B.shape[0] > _BATCH_ABOVE:
+            stream = torch.cuda.current_stream(B.device).cuda_stream
+            bt = pattern.batch(A, B.shape[0], opts.precision, stream)
+            _, reps = bt.solve([B], [X], options=opts, use_graph=False, stream=stream)
+            reports.extend(reps[0])
+            return X
         _, reps = A.solve_multi(B, X, options=opts)
         reports.extend(reps)
         return X
@@ -73,7 +109,7 @@ class _SparseSolve(torch.autograd.Function):
         A = pattern.matrix(val)
         B = b.detach().reshape(-1, b.shape[-1]).contiguous()
         pattern.reports = []
-        X = _solve_all(A, B, opts, pattern.reports)
+        X = _solve_all(A, B, opts, pattern.reports, pattern)
         ctx.pattern, ctx.opts = pattern, opts
         ctx.save_for_backward(X)
         ctx.bshape = b.shape
@@ -85,7 +121,7 @@ class _SparseSolve(torch.autograd.Function):
         pattern, opts = ctx.pattern, ctx.opts
         G = gx.detach().reshape(X.shape).contiguous()
         AT = pattern.adjoint()
-        lam = _solve_all(AT, G, opts, pattern.reports)
+        lam = _solve_all(AT, G, opts, pattern.reports, pattern)
         grad_val = grad_b = None
         if ctx.needs_input_grad[0]:
             grad_val = pattern._A.value_grad(lam, X)

@@ -73,6 +73,33 @@ def test_autograd_cg_matches_dense_gradient(mf, cuda, precision, tol, rtol):
     np.testing.assert_allclose(val.grad.cpu().numpy(), gval_ref, rtol=0, atol=rtol * np.abs(gval_ref).max())
 
 
+@pytest.mark.parametrize("precision,tol,rtol", [("fp64", 1e-12, 1e-7), ("mixed", 1e-10, 1e-5)])
+def test_autograd_cg_many_rhs_batch_matches_dense_gradient(mf, cuda, precision, tol, rtol):
+    """More than 8 right-hand sides go through the pattern's tuned one-system
+    batch, forward and adjoint (the symmetric adjoint reuses the forward's
+    batch); gradients against the dense FP64 ones, summed over the columns."""
+    from millefeuille import matrices as M
+    from millefeuille.autograd import SolvePattern, sparse_solve
+    A, B, Xt, _ = M.aniso2d_grf(32, seed=4, corr=8.0, nrhs=12)
+    rp, ci = _dev(A.rowptr), _dev(A.colidx)
+    pat = SolvePattern(rp, ci, A.n, symmetric=True)
+    val = _dev(A.val).requires_grad_(True)
+    bt = _dev(B).requires_grad_(True)
+    x = sparse_solve(rp, ci, val, bt, method="cg", precision=precision, tol=tol, pattern=pat)
+    ((x - _dev(Xt)) ** 2).sum().backward()
+    assert len(pat.reports) == 24 and all("item_blocks" in r for r in pat.reports)
+    assert all(r["converged"] and r["relres_true"] <= tol for r in pat.reports)
+    assert len(pat._batches) == 1
+    D = A.to_scipy().toarray()
+    X = np.linalg.solve(D, B.T).T
+    L = np.linalg.solve(D.T, 2.0 * (X - Xt).T).T
+    gval = -np.einsum("ke,ke->e", L[:, _rows(A)], X[:, A.colidx])
+    np.testing.assert_allclose(x.detach().cpu().numpy(), X, rtol=0, atol=rtol * np.abs(X).max())
+    np.testing.assert_allclose(bt.grad.cpu().numpy(), L, rtol=0, atol=rtol * np.abs(L).max())
+    np.testing.assert_allclose(val.grad.cpu().numpy(), gval, rtol=0, atol=rtol * np.abs(gval).max())
+    pat.close_batches()
+
+
 def test_autograd_cg_central_differences(mf, cuda):
     import torch
     from millefeuille import matrices as M
