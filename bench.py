@@ -472,6 +472,13 @@ def fwd_adjoint(dev, nrhs):
                    "iterations_forward_mean": round(sum(r["iterations"] for r in fwd_reps) / len(fwd_reps), 1),
                    "iterations_adjoint_mean": round(sum(r["iterations"] for r in adj_reps) / len(adj_reps), 1),
                    "relres_true_max": max(r["relres_true"] for r in fwd_reps + adj_reps),
+                   # more than 8 columns run as a one-system batch: its kernel time per solve
+                   # (the rest of forward_ms is tiling the new values and setting the batch up)
+                   "batch_config": [list(v) for v in pat._configs.values()],
+                   "forward_batch_kernel_ms": (round(fwd_reps[0]["time_ms"], 3)
+                                               if "item_blocks" in fwd_reps[0] else None),
+                   "adjoint_batch_kernel_ms": (round(adj_reps[0]["time_ms"], 3)
+                                               if "item_blocks" in adj_reps[0] else None),
                    "grad_val_norm": float(val.grad.norm()), "grad_b_norm": float(bt.grad.norm())}
     return res
 

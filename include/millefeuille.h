@@ -259,6 +259,12 @@ int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_o
  *                  full solve's tail of long items); *chosen_cap (nullable) gets
  *                  the right-hand sides per item (grid_blocks in the reports
  *                  shows the blocks).
+ * mf_batch_configure sets the right-hand sides per item (1, 2, 4 or 8) and the
+ *                  blocks per SM (1, or 2 for items of up to 4 columns where two
+ *                  blocks fit) without timing runs, e.g. to reuse what
+ *                  mf_batch_tune chose for a batch of the same shapes (new
+ *                  values, same sizes); MF_ERR_INVALID for other pairs.
+ * mf_batch_config  reads the current pair.
  * mf_batch_solve   B[k] / X[k]: DEVICE arrays of nrhs[k] x n_k doubles (one
  *                  vector after another).  reports (nullable): sum(nrhs)
  *                  records, system by system; time_ms is the whole batch's;
@@ -273,6 +279,8 @@ int mf_solve_multi(mf_matrix A, int nrhs, const double *B, double *X, const mf_o
 typedef struct mf_batch_s *mf_batch;
 int mf_batch_create(mf_batch *out, int nsys, const mf_matrix *systems, const int *nrhs, void *stream);
 int mf_batch_tune(mf_batch b, int precision, int iters, int *chosen_cap, void *stream);
+int mf_batch_configure(mf_batch b, int cap, int blocks_per_sm, void *stream);
+int mf_batch_config(mf_batch b, int *cap, int *blocks_per_sm);
 int mf_batch_solve(mf_batch b, const double *const *B, double *const *X, const mf_options *opt,
                    mf_report *reports, int use_graph, void *stream);
 int mf_batch_destroy(mf_batch b);

@@ -400,6 +400,19 @@ extern "C" int mf_batch_tune(mf_batch b, int precision, int iters, int *chosen_c
     return mf_batch_tune_impl(b, precision, iters, chosen_cap, (cudaStream_t)stream);
 }
 
+extern "C" int mf_batch_configure(mf_batch b, int cap, int blocks_per_sm, void *stream)
+{
+    if (!b) return MF_ERR_INVALID;
+    return mf_batch_configure_impl(b, cap, blocks_per_sm, (cudaStream_t)stream);
+}
+
+extern "C" int mf_batch_config(mf_batch b, int *cap, int *blocks_per_sm)
+{
+    if (!b) return MF_ERR_INVALID;
+    mf_batch_config_impl(b, cap, blocks_per_sm);
+    return MF_SUCCESS;
+}
+
 extern "C" int mf_batch_solve(mf_batch b, const double *const *B, double *const *X, const mf_options *opt,
                               mf_report *reports, int use_graph, void *stream)
 {

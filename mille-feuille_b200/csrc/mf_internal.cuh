@@ -160,6 +160,8 @@ int mf_batch_create_impl(mf_batch_s **out, int nsys, mf_matrix_s *const *systems
 int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *Xd, const mf_options *opt,
                         mf_report *reps, int use_graph, cudaStream_t s);
 int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cudaStream_t s);
+int mf_batch_configure_impl(mf_batch_s *b, int cap, int lb, cudaStream_t s);
+void mf_batch_config_impl(const mf_batch_s *b, int *cap, int *lb);
 void mf_batch_destroy_impl(mf_batch_s *b);
 int mf_batch_schedule_impl(int nitems, const double *cost, const int *tilem, int grid, int *team, int *bptr,
                            int *blist, int *queue, int *nqueue);

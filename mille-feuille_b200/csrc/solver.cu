@@ -3829,6 +3829,23 @@ int mf_batch_solve_impl(mf_batch_s *b, const double *const *Bd, double *const *X
 
 // Right-hand sides per work item chosen by timing: each candidate cap runs
 // `iters` fixed iterations of the real batch with all-ones right-hand sides.
+// A given (columns per item, blocks per SM), e.g. what mf_batch_tune chose for
+// a batch of the same systems' shapes: the same item build, no timing runs.
+int mf_batch_configure_impl(mf_batch_s *b, int cap, int lb, cudaStream_t s)
+{
+    BatchImpl &B = b->impl;
+    if (cap != 1 && cap != 2 && cap != 4 && cap != 8) return MF_ERR_INVALID;
+    // two blocks per SM only for items of up to 4 columns, as the tuner's candidates
+    if (lb != 1 && !(lb == 2 && cap <= 4 && B.max_res[2] >= 1)) return MF_ERR_INVALID;
+    return batch_build_items(B, cap, lb, s ? s : B.own);
+}
+
+void mf_batch_config_impl(const mf_batch_s *b, int *cap, int *lb)
+{
+    if (cap) *cap = b->impl.cap;
+    if (lb) *lb = b->impl.lb;
+}
+
 int mf_batch_tune_impl(mf_batch_s *b, int precision, int iters, int *chosen, cudaStream_t s)
 {
     BatchImpl &B = b->impl;

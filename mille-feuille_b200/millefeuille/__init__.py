@@ -319,6 +319,19 @@ class Batch:
               "mf_batch_tune")
         return cap.value
 
+    def configure(self, cap, blocks_per_sm=1, stream=None) -> None:
+        """Right-hand sides per work item and blocks per SM without timing runs
+        (mf_batch_configure), e.g. a pair config() read after tune() on a batch
+        of the same shapes."""
+        check(_lib.load().mf_batch_configure(self._h, int(cap), int(blocks_per_sm),
+                                             C.c_void_p(stream) if stream else None), "mf_batch_configure")
+
+    def config(self):
+        """(right-hand sides per item, blocks per SM) now in use (mf_batch_config)."""
+        cap, lb = C.c_int(), C.c_int()
+        check(_lib.load().mf_batch_config(self._h, C.byref(cap), C.byref(lb)), "mf_batch_config")
+        return cap.value, lb.value
+
     def solve(self, Bs, Xs=None, options: Options | None = None, use_graph=True, stream=None, **kw):
         """Bs: CUDA float64 tensors of shape (nrhs_k, n_k).  Returns (Xs, reports)
         with reports[k] the list of system k's per-column report dicts."""

@@ -74,7 +74,8 @@ EXPORTED = [
     "bicgstab_inc", "mf_read_matrix", "mf_write_cbd", "mf_free_host", "mf_options_default", "mf_matrix_create",
     "mf_matrix_destroy", "mf_matrix_get_info", "mf_tile_array_bytes", "mf_tile_export", "mf_solve", "mf_spmv",
     "mf_debug_ref_labels", "mf_build_arch", "mf_spmv_noalloc", "mf_value_grad", "mf_matrix_create_transposed",
-    "mf_solve_multi", "mf_batch_create", "mf_batch_tune", "mf_batch_solve", "mf_batch_destroy",
+    "mf_solve_multi", "mf_batch_create", "mf_batch_tune", "mf_batch_configure", "mf_batch_config",
+    "mf_batch_solve", "mf_batch_destroy",
     "mf_batch_partition", "mf_batch_schedule", "mf_debug_spmv_tiles", "mf_debug_solver_labels",
     "mf_dropin_last_report", "mf_debug_spmm",
 ]
@@ -106,6 +107,8 @@ def load() -> C.CDLL:
     L.mf_solve_multi.argtypes = [vp, C.c_int, vp, vp, C.POINTER(Options), C.POINTER(Report), C.c_int, vp]
     L.mf_batch_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp), C.POINTER(C.c_int), vp]
     L.mf_batch_tune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int), vp]
+    L.mf_batch_configure.argtypes = [vp, C.c_int, C.c_int, vp]
+    L.mf_batch_config.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.mf_batch_solve.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(Options), C.POINTER(Report), C.c_int,
                                  vp]
     L.mf_batch_destroy.argtypes = [vp]

@@ -38,7 +38,8 @@ class SolvePattern:
         self._key = None
         self._A = None
         self._AT = None
-        self._batches = {}          # (handle, nrhs, precision) -> tuned one-system Batch
+        self._batches = {}          # (handle, nrhs, precision) -> one-system Batch of the current values
+        self._configs = {}          # (rows, cols, nrhs, precision) -> (columns per item, blocks per SM)
         self.reports = []           # per-solve reports of the last forward / backward
 
     def matrix(self, val) -> Matrix:
@@ -58,14 +59,21 @@ class SolvePattern:
         return self._AT
 
     def batch(self, A: Matrix, nrhs: int, precision: int, stream) -> Batch:
-        """The one-system batch of A with nrhs right-hand sides, created and
-        tuned (mf_batch_tune: columns per work item, blocks per SM) on first
-        use and kept until the values change."""
+        """The one-system batch of A with nrhs right-hand sides, kept until the
+        values change.  The first batch of a column count and precision is
+        tuned (mf_batch_tune: columns per work item, blocks per SM); later ones
+        (new values, same pattern and sizes) take the same pair
+        (mf_batch_configure) without timing runs."""
         key = (id(A), int(nrhs), int(precision))
         bt = self._batches.get(key)
         if bt is None:
             bt = Batch([A], [int(nrhs)], stream=stream)
-            bt.tune(int(precision), stream=stream)
+            ckey = (A.info["n_rows"], A.info["n_cols"], key[1], key[2])
+            if ckey in self._configs:
+                bt.configure(*self._configs[ckey], stream=stream)
+            else:
+                bt.tune(key[2], stream=stream)
+                self._configs[ckey] = bt.config()
             self._batches[key] = bt
         return bt
 

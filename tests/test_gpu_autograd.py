@@ -78,6 +78,7 @@ def test_autograd_cg_many_rhs_batch_matches_dense_gradient(mf, cuda, precision, 
     """More than 8 right-hand sides go through the pattern's tuned one-system
     batch, forward and adjoint (the symmetric adjoint reuses the forward's
     batch); gradients against the dense FP64 ones, summed over the columns."""
+    import torch
     from millefeuille import matrices as M
     from millefeuille.autograd import SolvePattern, sparse_solve
     A, B, Xt, _ = M.aniso2d_grf(32, seed=4, corr=8.0, nrhs=12)
@@ -97,6 +98,15 @@ def test_autograd_cg_many_rhs_batch_matches_dense_gradient(mf, cuda, precision, 
     np.testing.assert_allclose(x.detach().cpu().numpy(), X, rtol=0, atol=rtol * np.abs(X).max())
     np.testing.assert_allclose(bt.grad.cpu().numpy(), L, rtol=0, atol=rtol * np.abs(L).max())
     np.testing.assert_allclose(val.grad.cpu().numpy(), gval, rtol=0, atol=rtol * np.abs(gval).max())
+    # new values tensor (same values): a new handle and batch, configured from the
+    # pair tuned above without timing runs; the same kernels give the same bits
+    cfg = dict(pat._configs)
+    val2 = _dev(A.val).requires_grad_(True)
+    bt2 = _dev(B).requires_grad_(True)
+    x2 = sparse_solve(rp, ci, val2, bt2, method="cg", precision=precision, tol=tol, pattern=pat)
+    ((x2 - _dev(Xt)) ** 2).sum().backward()
+    assert pat._configs == cfg and len(cfg) == 1
+    assert torch.equal(x2, x) and torch.equal(val2.grad, val.grad) and torch.equal(bt2.grad, bt.grad)
     pat.close_batches()
 
 

@@ -61,6 +61,22 @@ def test_batch_graph_replay_and_tuning(mf, cuda, systems):
     for (kind, side, A, B), X, rk in zip(systems, Xt, rt):
         for c in range(B.shape[0]):
             assert rk[c]["converged"] and _relres(A, X.cpu().numpy()[c], B[c]) <= 1.0001e-8
+    # the tuned pair, read back and given to a new batch of the same systems
+    # without timing runs: the same items and kernels, the same bits
+    cfg = batch.config()
+    assert cfg[0] == cap and cfg[1] in (1, 2)
+    for bad in ((3, 1), (0, 1), (8, 2), (4, 3)):
+        with pytest.raises(mf.MFError):
+            batch.configure(*bad)
+    assert batch.config() == cfg
+    other = mf.Batch(mats, [B.shape[0] for B in Bs])
+    other.configure(*cfg)
+    Xo, ro = other.solve(Bs, method="cg", precision="mixed", tol=1e-8)
+    assert other.config() == cfg
+    for a, b in zip(Xt, Xo):
+        assert torch.equal(a, b)
+    assert rt[0][0]["grid_blocks"] == ro[0][0]["grid_blocks"]
+    other.close()
 
 
 def test_batch_rejects_bad_input(mf, cuda, systems):
