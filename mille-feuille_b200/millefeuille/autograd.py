@@ -6,8 +6,8 @@ and for A's stored values.
 
 Forward: the single-kernel solve on device pointers -- for CG, mf_solve_multi
 (up to 8 right-hand sides in one launch) or, with more than 8, a one-system
-mf_batch tuned once per tiled handle and right-hand-side count (work items of
-up to 8 columns solved concurrently by teams of blocks); one mf_solve per
+mf_batch per tiled handle, tuned once per pattern and right-hand-side count
+(work items of up to 8 columns solved concurrently by teams of blocks); one mf_solve per
 column for BiCGSTAB.  Backward: the adjoint solve lambda = A^-T dL/dx with the same
 kernel -- on A itself for CG (A symmetric), on a transposed handle
 (mf_matrix_create_transposed) for BiCGSTAB -- then dL/db = lambda and
