@@ -558,11 +558,14 @@ def run_profile(args):
     import torch
     import millefeuille as mf
     dev = torch.device("cuda", 0)
+    kind = args.profile
+    if kind in ("spmm8", "batch32"):
+        run_profile_aniso(args, kind)
+        return
     A, b, _ = make_system()
     G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
     bd = torch.from_numpy(b).to(dev)
     xd = torch.zeros_like(bd)
-    kind = args.profile
     if kind.startswith("spmv"):
         prec = "fp64" if kind == "spmv_fp64" else "mixed"
         xs = torch.from_numpy(np.random.default_rng(7).uniform(-1, 1, A.n)).to(dev)
@@ -585,9 +588,45 @@ def run_profile(args):
                       "tile_uses": rep["tile_uses"]}))
 
 
+def run_profile_aniso(args, kind):
+    """Launches on the 512^2 anisotropic GRF matrix (seed 4) for ncu.
+    spmm8: --profile-iters launches each of the 8-column SpMM with FP16 stored
+    values on the CUDA cores (k_spmm_cc) and the tensor cores (k_spmm_tc),
+    uniform random X; the median CUDA-event time after 3 warm-up launches.
+    batch32: the one-system batch of 32 right-hand sides the autograd wrapper
+    uses (4 columns per item, one block per SM), --profile-iters fixed mixed CG
+    iterations, run twice (warm-up, then the launch to capture)."""
+    import numpy as np
+    import torch
+    import millefeuille as mf
+    from millefeuille import matrices as M
+    dev = torch.device("cuda", 0)
+    A, B, _, _ = M.aniso2d_grf(512, seed=4, nrhs=32)
+    G = mf.Matrix.from_csr(A.n, A.n, A.rowptr, A.colidx, A.val)
+    if kind == "spmm8":
+        X = torch.from_numpy(np.random.default_rng(7).uniform(-1, 1, (8, A.n))).to(dev)
+        out = {"profile": kind}
+        for tc in (False, True):
+            ts = [G.spmm8(X, tensor_cores=tc)[1] for _ in range(args.profile_iters)]
+            out["tensor_cores_us" if tc else "cuda_cores_us"] = round(1e3 * statistics.median(ts[3:] or ts), 2)
+        print(json.dumps(out))
+        return
+    bt = mf.Batch([G], [32])
+    bt.configure(4, 1)
+    Bd = torch.from_numpy(B).to(dev)
+    o = mf.default_options(precision="mixed", tol=TOL, max_iter=args.profile_iters, fixed_iters=1, replace_every=0)
+    for _ in range(2):
+        _, reps = bt.solve([Bd], options=o, use_graph=False)
+    r = reps[0][0]
+    print(json.dumps({"profile": kind, "iterations": r["iterations"], "kernel_ms": r["time_ms"],
+                      "grid": [r["grid_blocks"], r["threads_per_block"]], "item_blocks": r["item_blocks"]}))
+    bt.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["solve_fp64", "solve_mixed", "solve_mixed_tol", "spmv_fp64", "spmv_mixed"],
+    ap.add_argument("--profile", choices=["solve_fp64", "solve_mixed", "solve_mixed_tol", "spmv_fp64", "spmv_mixed",
+                                          "spmm8", "batch32"],
                     help="run one small launch of a kernel for an ncu capture and exit")
     ap.add_argument("--profile-iters", type=int, default=20)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
